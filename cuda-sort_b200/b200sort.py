@@ -1,0 +1,175 @@
+"""ctypes binding of the b200sort C ABI (include/b200sort.h).
+
+The library is the product; this module only loads it and forwards calls.
+There is no fallback: if libb200sort.so is missing the import of `lib()`
+raises, and every sort runs the CUDA kernels of that library.
+
+Device buffers are passed as integer device pointers (for example
+`tensor.data_ptr()` of a CUDA tensor) and streams as integer cudaStream_t
+handles (for example `torch.cuda.current_stream().cuda_stream`).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libb200sort.so")
+
+I32, I32_I32, U64, U64_I32 = 0, 1, 2, 3
+DTYPES = {"i32": I32, "i32_i32": I32_I32, "u64": U64, "u64_i32": U64_I32}
+STABLE = 1
+SORTED_CHECK = 2
+ELEM_BYTES = {I32: 4, I32_I32: 8, U64: 8, U64_I32: 16}
+
+# numpy views of the memory layouts
+NP_DTYPES = {
+    I32: np.dtype("<i4"),
+    I32_I32: np.dtype([("key", "<i4"), ("data", "<i4")]),
+    U64: np.dtype("<u8"),
+    U64_I32: np.dtype([("key", "<u8"), ("data", "<i4"), ("reserved", "<i4")]),
+}
+
+OK = 0
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED", 3: "CUDA", 4: "OUT_OF_MEMORY",
+                5: "TIMEOUT", 6: "BUDGET"}
+
+
+class Tile(ctypes.Structure):
+    _fields_ = [("log2_items", ctypes.c_int32), ("log2_lanes", ctypes.c_int32),
+                ("log2_warps", ctypes.c_int32), ("cta_threads", ctypes.c_int32)]
+
+    def as_tuple(self):
+        return (self.log2_items, self.log2_lanes, self.log2_warps)
+
+    def __repr__(self):
+        return "Tile(K=%d, lanes=%d, warps=%d, cta=%d)" % (
+            1 << self.log2_items, 1 << self.log2_lanes, 1 << self.log2_warps, self.cta_threads)
+
+
+class B200SortError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("b200sort %s: %s" % (STATUS_NAMES.get(status, status), message))
+        self.status = status
+
+
+_lib = None
+
+_SIGNATURES = {
+    "b200s_version": (ctypes.c_char_p, []),
+    "b200s_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "b200s_last_error": (ctypes.c_char_p, []),
+    "b200s_max_length": (ctypes.c_int32, [ctypes.c_int, ctypes.c_uint32]),
+    "b200s_tile_count": (ctypes.c_int32, [ctypes.c_int, ctypes.c_uint32]),
+    "b200s_tile_get": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.c_int32, ctypes.POINTER(Tile)]),
+    "b200s_default_tile": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.c_int32, ctypes.POINTER(Tile)]),
+    "b200s_load_tile_table": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32)]),
+    "b200s_sort_packed": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                         ctypes.c_int64, ctypes.c_uint32, ctypes.POINTER(Tile),
+                                         ctypes.c_void_p]),
+    "b200s_session_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32]),
+    "b200s_session_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "b200s_sort_packed_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32]),
+}
+
+
+def lib():
+    """Load libb200sort.so once and declare the C signatures."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libb200sort.so not built at %s (run __graft_entry__.build())" % LIB_PATH)
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def declare(name, restype, argtypes):
+    """Declare an additional entry point of the library (used by sibling modules)."""
+    fn = getattr(lib(), name)
+    fn.restype = restype
+    fn.argtypes = argtypes
+    return fn
+
+
+def check(status):
+    if status != OK:
+        raise B200SortError(status, lib().b200s_last_error().decode())
+    return status
+
+
+def version():
+    return lib().b200s_version().decode()
+
+
+def max_length(dtype, flags=0):
+    return lib().b200s_max_length(dtype, flags)
+
+
+def tiles(dtype, flags=0):
+    out = []
+    for i in range(lib().b200s_tile_count(dtype, flags)):
+        t = Tile()
+        check(lib().b200s_tile_get(dtype, flags, i, ctypes.byref(t)))
+        out.append(t)
+    return out
+
+
+def default_tile(dtype, n, flags=0):
+    t = Tile()
+    check(lib().b200s_default_tile(dtype, flags, n, ctypes.byref(t)))
+    return t
+
+
+def load_tile_table(path):
+    applied = ctypes.c_int32(0)
+    check(lib().b200s_load_tile_table(path.encode(), ctypes.byref(applied)))
+    return applied.value
+
+
+def sort_packed(dtype, d_in, d_out, n, arrays, flags=0, tile=None, stream=0):
+    """Sort `arrays` packed arrays of n elements from device pointer d_in to d_out."""
+    tp = ctypes.byref(tile) if tile is not None else None
+    return check(lib().b200s_sort_packed(dtype, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out), n, arrays,
+                                         flags, tp, ctypes.c_void_p(stream)))
+
+
+def sort_packed_status(dtype, d_in, d_out, n, arrays, flags=0, tile=None, stream=0):
+    """Like sort_packed but returns the raw status code instead of raising."""
+    tp = ctypes.byref(tile) if tile is not None else None
+    return lib().b200s_sort_packed(dtype, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out), n, arrays, flags,
+                                   tp, ctypes.c_void_p(stream))
+
+
+class Session:
+    """Host-buffer sorting: copies in, sorts on the device, copies out."""
+
+    def __init__(self, device=0):
+        self._h = ctypes.c_void_p()
+        check(lib().b200s_session_create(ctypes.byref(self._h), device))
+
+    def sort_host(self, dtype, h_in, h_out, n, arrays, flags=0):
+        return check(lib().b200s_sort_packed_host(self._h, dtype, ctypes.c_void_p(h_in), ctypes.c_void_p(h_out),
+                                                  n, arrays, flags))
+
+    def close(self):
+        if self._h:
+            lib().b200s_session_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

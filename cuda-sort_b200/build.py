@@ -1,0 +1,70 @@
+"""Build recipe for the b200sort CUDA library (sm_100a only).
+
+Compiles every translation unit under csrc/ to an object with nvcc, in
+parallel, and links them into libb200sort.so beside this file.  Objects are
+rebuilt only when a source or header is newer than the object.
+"""
+import concurrent.futures
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libb200sort.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+         "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+
+
+def _sources():
+    return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+
+
+def _headers_mtime():
+    newest = 0.0
+    for d in (CSRC, os.path.join(ROOT, "include")):
+        for f in os.listdir(d):
+            if f.endswith((".cuh", ".h", ".hpp")):
+                newest = max(newest, os.path.getmtime(os.path.join(d, f)))
+    return newest
+
+
+def _compile(src, extra):
+    obj = os.path.join(OBJ, src[:-3] + ".o")
+    path = os.path.join(CSRC, src)
+    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(path), _headers_mtime()):
+        return obj, None
+    cmd = [NVCC] + ARCH + FLAGS + extra + ["-c", path, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        return obj, "$ " + " ".join(cmd) + "\n" + r.stdout + r.stderr
+    return obj, None
+
+
+def build(verbose=False, extra=None, jobs=None):
+    """Compile csrc/*.cu for sm_100a and link libb200sort.so; return its path."""
+    os.makedirs(OBJ, exist_ok=True)
+    extra = list(extra or [])
+    jobs = jobs or max(1, min(len(_sources()), os.cpu_count() or 1))
+    with concurrent.futures.ThreadPoolExecutor(jobs) as ex:
+        results = list(ex.map(lambda s: _compile(s, extra), _sources()))
+    errors = [e for _, e in results if e]
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
+    objs = [o for o, _ in results]
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+    if verbose:
+        print("built", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, extra=sys.argv[1:])

@@ -1,0 +1,413 @@
+// C ABI of the batched sort: argument checking, tile selection, launches,
+// and the host-buffer (end-to-end) entry point.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "b200sort.h"
+#include "registry.h"
+
+namespace b200s {
+
+namespace {
+thread_local std::string g_error;
+}
+
+b200s_status set_error(b200s_status s, const std::string& msg) {
+    g_error = msg;
+    return s;
+}
+
+b200s_status cuda_error(cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return set_error(e == cudaErrorMemoryAllocation ? B200S_ERR_OUT_OF_MEMORY : B200S_ERR_CUDA, m);
+}
+
+void clear_error() { g_error.clear(); }
+
+size_t elem_bytes(int dtype) {
+    switch (dtype) {
+        case B200S_I32: return 4;
+        case B200S_I32_I32: return 8;
+        case B200S_U64: return 8;
+        case B200S_U64_I32: return 16;
+        default: return 0;
+    }
+}
+
+// Keys alone are indistinguishable when equal: stable and unstable coincide.
+int effective_stable(int dtype, uint32_t flags) {
+    return ((flags & B200S_STABLE) && (dtype == B200S_I32_I32 || dtype == B200S_U64_I32)) ? 1 : 0;
+}
+
+int ceil_log2(long long n) {
+    int b = 0;
+    while ((1LL << b) < n) ++b;
+    return b;
+}
+
+const std::vector<KernelEntry>& registry() {
+    static std::vector<KernelEntry> all = [] {
+        std::vector<KernelEntry> v;
+        register_i32(v);
+        register_rec(v);
+        register_u64(v);
+        return v;
+    }();
+    return all;
+}
+
+namespace {
+
+constexpr int kMaxLog2W = 20;
+
+struct DefaultTable {
+    int pick[4][2][kMaxLog2W + 1];
+};
+
+std::mutex g_table_mutex;
+
+int preferred_lk(int dtype) { return dtype == B200S_I32 ? 5 : 4; }
+
+DefaultTable build_defaults() {
+    DefaultTable t;
+    const auto& reg = registry();
+    for (int d = 0; d < 4; ++d)
+        for (int s = 0; s < 2; ++s)
+            for (int w = 0; w <= kMaxLog2W; ++w) {
+                int best = -1, best_score = -1;
+                for (size_t i = 0; i < reg.size(); ++i) {
+                    const KernelEntry& e = reg[i];
+                    if (e.dtype != d || e.stable != s || e.log2w != w) continue;
+                    // Prefer the type's preferred register depth, then fewer
+                    // warps per array (fewer barriers).
+                    int score = (e.lk == preferred_lk(d) ? 1000 : 100 * e.lk) - 10 * e.lw;
+                    if (score > best_score) {
+                        best_score = score;
+                        best = int(i);
+                    }
+                }
+                t.pick[d][s][w] = best;
+            }
+    return t;
+}
+
+DefaultTable& table() {
+    static DefaultTable t = build_defaults();
+    return t;
+}
+
+// Entry for arrays of length n: the tabled tile for the smallest compiled
+// working length >= n.
+int lookup_default(int dtype, int stable, long long n) {
+    std::lock_guard<std::mutex> lock(g_table_mutex);
+    const DefaultTable& t = table();
+    for (int w = std::max(0, ceil_log2(n)); w <= kMaxLog2W; ++w)
+        if (t.pick[dtype][stable][w] >= 0) return t.pick[dtype][stable][w];
+    return -1;
+}
+
+int lookup_tile(int dtype, int stable, const b200s_tile& tile) {
+    const auto& reg = registry();
+    for (size_t i = 0; i < reg.size(); ++i) {
+        const KernelEntry& e = reg[i];
+        if (e.dtype == dtype && e.stable == stable && e.lk == tile.log2_items &&
+            e.lg == tile.log2_lanes && e.lw == tile.log2_warps)
+            return int(i);
+    }
+    return -1;
+}
+
+void fill_tile(const KernelEntry& e, b200s_tile* out) {
+    out->log2_items = e.lk;
+    out->log2_lanes = e.lg;
+    out->log2_warps = e.lw;
+    out->cta_threads = e.cta;
+}
+
+bool valid_dtype(int d) { return d >= 0 && d <= 3; }
+
+}  // namespace
+
+// Launch the packed kernel of registry entry `idx`.
+b200s_status launch_packed(int idx, const void* in, void* out, int n, long long arrays,
+                           cudaStream_t st) {
+    const KernelEntry& e = registry()[size_t(idx)];
+    long long grid = (arrays + e.apc - 1) / e.apc;
+    grid = std::min<long long>(grid, 0x7fffffffLL);
+    cudaError_t err = e.launch(in, out, n, arrays, grid, st);
+    if (err != cudaSuccess) return cuda_error(err, "sort kernel launch");
+    return B200S_OK;
+}
+
+int select_entry(int dtype, uint32_t flags, long long n, const b200s_tile* tile, b200s_status* st) {
+    const int stable = effective_stable(dtype, flags);
+    int idx;
+    if (tile) {
+        idx = lookup_tile(dtype, stable, *tile);
+        if (idx < 0) {
+            *st = set_error(B200S_ERR_UNSUPPORTED, "no compiled kernel for the requested tile");
+            return -1;
+        }
+        if ((1LL << registry()[size_t(idx)].log2w) < n) {
+            *st = set_error(B200S_ERR_UNSUPPORTED, "tile working length is shorter than n");
+            return -1;
+        }
+    } else {
+        idx = lookup_default(dtype, stable, n);
+        if (idx < 0) {
+            *st = set_error(B200S_ERR_UNSUPPORTED, "array length exceeds the largest compiled tile");
+            return -1;
+        }
+    }
+    *st = B200S_OK;
+    return idx;
+}
+
+}  // namespace b200s
+
+using namespace b200s;
+
+extern "C" {
+
+const char* b200s_version(void) { return "b200sort 0.1.0 (sm_100a)"; }
+
+const char* b200s_status_string(b200s_status s) {
+    switch (s) {
+        case B200S_OK: return "ok";
+        case B200S_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case B200S_ERR_UNSUPPORTED: return "unsupported";
+        case B200S_ERR_CUDA: return "CUDA error";
+        case B200S_ERR_OUT_OF_MEMORY: return "out of memory";
+        case B200S_ERR_TIMEOUT: return "timeout";
+        case B200S_ERR_BUDGET: return "over budget";
+    }
+    return "unknown status";
+}
+
+const char* b200s_last_error(void) { return b200s::g_error.c_str(); }
+
+int32_t b200s_max_length(b200s_dtype dtype, uint32_t flags) {
+    if (!valid_dtype(dtype)) return 0;
+    const int stable = effective_stable(dtype, flags);
+    int best = 0;
+    for (const KernelEntry& e : registry())
+        if (e.dtype == dtype && e.stable == stable) best = std::max(best, e.log2w);
+    return best ? int32_t(1) << best : 0;
+}
+
+int32_t b200s_tile_count(b200s_dtype dtype, uint32_t flags) {
+    if (!valid_dtype(dtype)) return 0;
+    const int stable = effective_stable(dtype, flags);
+    int c = 0;
+    for (const KernelEntry& e : registry())
+        if (e.dtype == dtype && e.stable == stable) ++c;
+    return c;
+}
+
+b200s_status b200s_tile_get(b200s_dtype dtype, uint32_t flags, int32_t index, b200s_tile* out) {
+    if (!valid_dtype(dtype) || !out || index < 0)
+        return set_error(B200S_ERR_INVALID_ARGUMENT, "b200s_tile_get: bad argument");
+    const int stable = effective_stable(dtype, flags);
+    int c = 0;
+    for (const KernelEntry& e : registry()) {
+        if (e.dtype != dtype || e.stable != stable) continue;
+        if (c++ == index) {
+            fill_tile(e, out);
+            return B200S_OK;
+        }
+    }
+    return set_error(B200S_ERR_INVALID_ARGUMENT, "b200s_tile_get: index out of range");
+}
+
+b200s_status b200s_default_tile(b200s_dtype dtype, uint32_t flags, int32_t n, b200s_tile* out) {
+    if (!valid_dtype(dtype) || !out || n < 0)
+        return set_error(B200S_ERR_INVALID_ARGUMENT, "b200s_default_tile: bad argument");
+    b200s_status st;
+    const int idx = select_entry(dtype, flags, std::max(1, n), nullptr, &st);
+    if (idx < 0) return st;
+    fill_tile(registry()[size_t(idx)], out);
+    return B200S_OK;
+}
+
+b200s_status b200s_load_tile_table(const char* path, int32_t* applied) {
+    if (!path) return set_error(B200S_ERR_INVALID_ARGUMENT, "b200s_load_tile_table: null path");
+    std::ifstream f(path);
+    if (!f) return set_error(B200S_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path);
+    std::string line;
+    int rows = 0, lineno = 0;
+    std::vector<std::array<int, 3>> updates;  // dtype*2+stable, log2w, index
+    while (std::getline(f, line)) {
+        ++lineno;
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line.resize(hash);
+        if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
+        std::replace(line.begin(), line.end(), ',', ' ');
+        std::istringstream ss(line);
+        int d, fl, w, lk, lg, lw;
+        if (!(ss >> d >> fl >> w >> lk >> lg >> lw))
+            return set_error(B200S_ERR_INVALID_ARGUMENT,
+                             "tile table line " + std::to_string(lineno) + ": expected 6 integers");
+        if (!valid_dtype(d) || w < 0 || w > 20)
+            return set_error(B200S_ERR_INVALID_ARGUMENT,
+                             "tile table line " + std::to_string(lineno) + ": bad dtype or log2_w");
+        const int stable = effective_stable(d, uint32_t(fl));
+        const b200s_tile tile{lk, lg, lw, 0};
+        const int idx = lookup_tile(d, stable, tile);
+        if (idx < 0 || registry()[size_t(idx)].log2w < w)
+            return set_error(B200S_ERR_UNSUPPORTED,
+                             "tile table line " + std::to_string(lineno) + ": tile not compiled or too short");
+        updates.push_back({d * 2 + stable, w, idx});
+        ++rows;
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_table_mutex);
+        DefaultTable& t = table();
+        for (const auto& u : updates) t.pick[u[0] / 2][u[0] % 2][u[1]] = u[2];
+    }
+    if (applied) *applied = rows;
+    clear_error();
+    return B200S_OK;
+}
+
+b200s_status b200s_sort_packed(b200s_dtype dtype, const void* d_in, void* d_out, int32_t n,
+                               int64_t arrays, uint32_t flags, const b200s_tile* tile,
+                               void* stream) {
+    if (!valid_dtype(dtype)) return set_error(B200S_ERR_INVALID_ARGUMENT, "unknown dtype");
+    if (n < 0 || arrays < 0) return set_error(B200S_ERR_INVALID_ARGUMENT, "negative n or arrays");
+    if (flags & ~(B200S_STABLE | B200S_SORTED_CHECK))
+        return set_error(B200S_ERR_INVALID_ARGUMENT, "unknown flag bits");
+    if (n == 0 || arrays == 0) return B200S_OK;
+    if (!d_in || !d_out) return set_error(B200S_ERR_INVALID_ARGUMENT, "null buffer");
+    b200s_status st;
+    const int idx = select_entry(dtype, flags, n, tile, &st);
+    if (idx < 0) return st;
+    return launch_packed(idx, d_in, d_out, n, arrays, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"
+
+// ---- sessions: host buffers in, host buffers out -------------------------------
+struct b200s_session {
+    int device = 0;
+    static constexpr int kDepth = 3;
+    cudaStream_t stream[kDepth] = {};
+    void* dbuf[kDepth] = {};
+    size_t capacity = 0;  // bytes per buffer
+};
+
+namespace {
+
+void release_buffers(b200s_session* s) {
+    for (int i = 0; i < b200s_session::kDepth; ++i) {
+        if (s->dbuf[i]) cudaFree(s->dbuf[i]);
+        s->dbuf[i] = nullptr;
+    }
+    s->capacity = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+b200s_status b200s_session_create(b200s_session** out, int32_t device) {
+    if (!out) return set_error(B200S_ERR_INVALID_ARGUMENT, "null session pointer");
+    *out = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    auto* s = new b200s_session();
+    s->device = device;
+    for (int i = 0; i < b200s_session::kDepth; ++i) {
+        e = cudaStreamCreateWithFlags(&s->stream[i], cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            for (int j = 0; j < i; ++j) cudaStreamDestroy(s->stream[j]);
+            delete s;
+            return cuda_error(e, "cudaStreamCreate");
+        }
+    }
+    *out = s;
+    return B200S_OK;
+}
+
+b200s_status b200s_session_destroy(b200s_session* s) {
+    if (!s) return B200S_OK;
+    cudaSetDevice(s->device);
+    for (int i = 0; i < b200s_session::kDepth; ++i) {
+        if (s->stream[i]) {
+            cudaStreamSynchronize(s->stream[i]);
+            cudaStreamDestroy(s->stream[i]);
+        }
+    }
+    release_buffers(s);
+    delete s;
+    return B200S_OK;
+}
+
+b200s_status b200s_sort_packed_host(b200s_session* s, b200s_dtype dtype, const void* h_in,
+                                    void* h_out, int32_t n, int64_t arrays, uint32_t flags) {
+    if (!s) return set_error(B200S_ERR_INVALID_ARGUMENT, "null session");
+    if (!valid_dtype(dtype)) return set_error(B200S_ERR_INVALID_ARGUMENT, "unknown dtype");
+    if (n < 0 || arrays < 0) return set_error(B200S_ERR_INVALID_ARGUMENT, "negative n or arrays");
+    if (flags & ~(B200S_STABLE | B200S_SORTED_CHECK))
+        return set_error(B200S_ERR_INVALID_ARGUMENT, "unknown flag bits");
+    if (n == 0 || arrays == 0) return B200S_OK;
+    if (!h_in || !h_out) return set_error(B200S_ERR_INVALID_ARGUMENT, "null buffer");
+    b200s_status st;
+    const int idx = select_entry(dtype, flags, n, nullptr, &st);
+    if (idx < 0) return st;
+    cudaError_t e = cudaSetDevice(s->device);
+    if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+
+    // Chunks of whole arrays, about 2 MB each: small enough that the last
+    // chunk's sort and copy-back are a short tail, large enough that copy
+    // latency is amortised.
+    const size_t eb = elem_bytes(dtype);
+    const size_t array_bytes = size_t(n) * eb;
+    const long long per_chunk = std::max<long long>(1, (long long)((2u << 20) / array_bytes));
+    const size_t need = size_t(std::min<long long>(per_chunk, arrays)) * array_bytes;
+    if (need > s->capacity) {
+        for (int i = 0; i < b200s_session::kDepth; ++i)
+            if (s->stream[i]) cudaStreamSynchronize(s->stream[i]);
+        release_buffers(s);
+        for (int i = 0; i < b200s_session::kDepth; ++i) {
+            e = cudaMalloc(&s->dbuf[i], need);
+            if (e != cudaSuccess) {
+                release_buffers(s);
+                return cuda_error(e, "session buffer allocation");
+            }
+        }
+        s->capacity = need;
+    }
+    const char* src = static_cast<const char*>(h_in);
+    char* dst = static_cast<char*>(h_out);
+    long long chunk = 0;
+    for (long long first = 0; first < arrays; first += per_chunk, ++chunk) {
+        const long long count = std::min<long long>(per_chunk, arrays - first);
+        const size_t bytes = size_t(count) * array_bytes;
+        const int k = int(chunk % b200s_session::kDepth);
+        cudaStream_t stream = s->stream[k];
+        e = cudaMemcpyAsync(s->dbuf[k], src + size_t(first) * array_bytes, bytes,
+                            cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return cuda_error(e, "host-to-device copy");
+        st = launch_packed(idx, s->dbuf[k], s->dbuf[k], n, count, stream);
+        if (st != B200S_OK) return st;
+        e = cudaMemcpyAsync(dst + size_t(first) * array_bytes, s->dbuf[k], bytes,
+                            cudaMemcpyDeviceToHost, stream);
+        if (e != cudaSuccess) return cuda_error(e, "device-to-host copy");
+    }
+    for (int i = 0; i < b200s_session::kDepth; ++i) {
+        e = cudaStreamSynchronize(s->stream[i]);
+        if (e != cudaSuccess) return cuda_error(e, "session synchronize");
+    }
+    return B200S_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,207 @@
+// Element types and their comparison rules for the batched bitonic sort.
+//
+// Memory layouts (what the caller's buffers hold):
+//   int32_t   keys only                                   4 B
+//   RecI32    {int32 key; int32 data;}  == IntAndData     8 B  (intanddata.hpp:9-11)
+//   uint64_t  keys only                                   8 B
+//   RecU64    {uint64 key; int32 data; int32 reserved;}  16 B  (AoS; reserved is written as 0)
+//
+// Register forms (what a thread holds while sorting) add an original-position
+// word in the stable mode, so that ties are broken by input order.
+//
+// Ordering follows the reference: records compare by key only
+// (intanddata.hpp:20-31) and, on the default path, a comparator keeps its own
+// element on ties: min(a,b) = b<a ? b : a, max(a,b) = a<b ? b : a
+// (cusort.hpp:460-472).  Padding uses the maximum key with a maximum payload
+// (cusort.hpp:257-271, intanddata.hpp:47-52).
+#pragma once
+#include <climits>
+#include <cstdint>
+
+namespace b200s {
+
+struct RecI32 {
+    int32_t key;
+    int32_t data;
+};
+struct __align__(16) RecU64 {
+    uint64_t key;
+    int32_t data;
+    int32_t reserved;
+};
+
+__device__ __forceinline__ uint32_t shfl_x(uint32_t v, int m) {
+    return __shfl_xor_sync(0xffffffffu, v, m);
+}
+__device__ __forceinline__ int32_t shfl_x(int32_t v, int m) {
+    return __shfl_xor_sync(0xffffffffu, v, m);
+}
+__device__ __forceinline__ uint64_t shfl_x(uint64_t v, int m) {
+    return __shfl_xor_sync(0xffffffffu, (unsigned long long)v, m);
+}
+
+// ---- int32 keys --------------------------------------------------------------
+struct ElemI32 {
+    using Mem = int32_t;
+    using Reg = int32_t;
+    static constexpr bool kStable = false;
+    static __device__ __forceinline__ Reg pad() { return INT32_MAX; }
+    static __device__ __forceinline__ Reg from_mem(Mem m, int) { return m; }
+    static __device__ __forceinline__ Mem to_mem(Reg r) { return r; }
+    static __device__ __forceinline__ Reg shfl(Reg v, int m) { return shfl_x(v, m); }
+    // Ascending compare-exchange of (lower, upper).  Equal keys are
+    // indistinguishable, so min/max is the keep-own rule.
+    static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
+        const Reg a = lo, b = hi;
+        lo = min(a, b);
+        hi = max(a, b);
+    }
+    // One side of a cross-thread compare-exchange: the upper side keeps the
+    // larger, the lower side the smaller.
+    static __device__ __forceinline__ Reg pick(Reg own, Reg other, bool upper) {
+        return upper ? max(own, other) : min(own, other);
+    }
+};
+
+// ---- uint64 keys -------------------------------------------------------------
+struct ElemU64 {
+    using Mem = uint64_t;
+    using Reg = uint64_t;
+    static constexpr bool kStable = false;
+    static __device__ __forceinline__ Reg pad() { return UINT64_MAX; }
+    static __device__ __forceinline__ Reg from_mem(Mem m, int) { return m; }
+    static __device__ __forceinline__ Mem to_mem(Reg r) { return r; }
+    static __device__ __forceinline__ Reg shfl(Reg v, int m) { return shfl_x(v, m); }
+    static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
+        const Reg a = lo, b = hi;
+        const bool sw = b < a;
+        lo = sw ? b : a;
+        hi = sw ? a : b;
+    }
+    static __device__ __forceinline__ Reg pick(Reg own, Reg other, bool upper) {
+        const bool take = upper ? (own < other) : (other < own);
+        return take ? other : own;
+    }
+};
+
+// ---- records: int32 key + int32 payload (IntAndData) ------------------------
+struct RegRecI32 {
+    int32_t key;
+    int32_t data;
+};
+struct ElemRecI32 {
+    using Mem = RecI32;
+    using Reg = RegRecI32;
+    static constexpr bool kStable = false;
+    static __device__ __forceinline__ Reg pad() { return Reg{INT32_MAX, INT32_MAX}; }
+    static __device__ __forceinline__ Reg from_mem(Mem m, int) { return Reg{m.key, m.data}; }
+    static __device__ __forceinline__ Mem to_mem(Reg r) { return Mem{r.key, r.data}; }
+    static __device__ __forceinline__ Reg shfl(Reg v, int m) {
+        return Reg{shfl_x(v.key, m), shfl_x(v.data, m)};
+    }
+    static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
+        const Reg a = lo, b = hi;
+        const bool sw = b.key < a.key;          // strict: ties keep their places
+        lo.key = sw ? b.key : a.key;
+        lo.data = sw ? b.data : a.data;
+        hi.key = sw ? a.key : b.key;
+        hi.data = sw ? a.data : b.data;
+    }
+    static __device__ __forceinline__ Reg pick(Reg own, Reg other, bool upper) {
+        const bool take = upper ? (own.key < other.key) : (other.key < own.key);
+        return Reg{take ? other.key : own.key, take ? other.data : own.data};
+    }
+};
+
+// Stable mode for IntAndData: (key, original position) is unique, so the
+// network output equals a stable sort by key.
+struct RegRecI32S {
+    int32_t key;
+    int32_t data;
+    int32_t pos;
+};
+struct ElemRecI32S {
+    using Mem = RecI32;
+    using Reg = RegRecI32S;
+    static constexpr bool kStable = true;
+    static __device__ __forceinline__ Reg pad() { return Reg{INT32_MAX, INT32_MAX, INT32_MAX}; }
+    static __device__ __forceinline__ Reg from_mem(Mem m, int pos) { return Reg{m.key, m.data, pos}; }
+    static __device__ __forceinline__ Mem to_mem(Reg r) { return Mem{r.key, r.data}; }
+    static __device__ __forceinline__ Reg shfl(Reg v, int m) {
+        return Reg{shfl_x(v.key, m), shfl_x(v.data, m), shfl_x(v.pos, m)};
+    }
+    static __device__ __forceinline__ bool lt(const Reg& a, const Reg& b) {
+        return a.key < b.key || (a.key == b.key && a.pos < b.pos);
+    }
+    static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
+        const Reg a = lo, b = hi;
+        const bool sw = lt(b, a);
+        lo = sw ? b : a;
+        hi = sw ? a : b;
+    }
+    static __device__ __forceinline__ Reg pick(Reg own, Reg other, bool upper) {
+        const bool take = upper ? lt(own, other) : lt(other, own);
+        return take ? other : own;
+    }
+};
+
+// ---- records: uint64 key + int32 payload -------------------------------------
+struct RegRecU64 {
+    uint64_t key;
+    int32_t data;
+};
+struct ElemRecU64 {
+    using Mem = RecU64;
+    using Reg = RegRecU64;
+    static constexpr bool kStable = false;
+    static __device__ __forceinline__ Reg pad() { return Reg{UINT64_MAX, INT32_MAX}; }
+    static __device__ __forceinline__ Reg from_mem(Mem m, int) { return Reg{m.key, m.data}; }
+    static __device__ __forceinline__ Mem to_mem(Reg r) { return Mem{r.key, r.data, 0}; }
+    static __device__ __forceinline__ Reg shfl(Reg v, int m) {
+        return Reg{shfl_x(v.key, m), shfl_x(v.data, m)};
+    }
+    static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
+        const Reg a = lo, b = hi;
+        const bool sw = b.key < a.key;
+        lo = sw ? b : a;
+        hi = sw ? a : b;
+    }
+    static __device__ __forceinline__ Reg pick(Reg own, Reg other, bool upper) {
+        const bool take = upper ? (own.key < other.key) : (other.key < own.key);
+        return take ? other : own;
+    }
+};
+
+struct RegRecU64S {
+    uint64_t key;
+    int32_t data;
+    int32_t pos;
+};
+struct ElemRecU64S {
+    using Mem = RecU64;
+    using Reg = RegRecU64S;
+    static constexpr bool kStable = true;
+    static __device__ __forceinline__ Reg pad() { return Reg{UINT64_MAX, INT32_MAX, INT32_MAX}; }
+    static __device__ __forceinline__ Reg from_mem(Mem m, int pos) { return Reg{m.key, m.data, pos}; }
+    static __device__ __forceinline__ Mem to_mem(Reg r) { return Mem{r.key, r.data, 0}; }
+    static __device__ __forceinline__ Reg shfl(Reg v, int m) {
+        return Reg{shfl_x(v.key, m), shfl_x(v.data, m), shfl_x(v.pos, m)};
+    }
+    static __device__ __forceinline__ bool lt(const Reg& a, const Reg& b) {
+        return a.key < b.key || (a.key == b.key && a.pos < b.pos);
+    }
+    static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
+        const Reg a = lo, b = hi;
+        const bool sw = lt(b, a);
+        lo = sw ? b : a;
+        hi = sw ? a : b;
+    }
+    static __device__ __forceinline__ Reg pick(Reg own, Reg other, bool upper) {
+        const bool take = upper ? lt(own, other) : lt(other, own);
+        return take ? other : own;
+    }
+};
+
+// uint64 keys alone are totally ordered values: the stable mode changes nothing.
+
+}  // namespace b200s

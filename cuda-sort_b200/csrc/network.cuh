@@ -1,0 +1,217 @@
+// The reflection bitonic network, mapped onto registers, warp lanes and
+// shared memory of one B200 CTA.
+//
+// Network (same comparators as cusort_v6.hpp:90-142): for each stage span
+// S = 1, 2, ..., W/2, one reflection layer pairing index i with i ^ (2S-1),
+// then merge layers pairing i with i ^ d for d = S/2, ..., 1.  In every pair
+// the lower index receives the smaller element, and an exchange happens only
+// when the upper element is strictly smaller (the keep-own rule of
+// cusort.hpp:460-472).  Because of that rule, maximum-key padding placed after
+// the n valid elements never moves, so any power-of-two W >= n yields the
+// same output; the tile table is free to choose W.
+//
+// Mapping (blocked): the W-element working tile is held as K = 2^LK
+// consecutive elements per thread.  Index bits [0, LK) select a register,
+// bits [LK, LK+LG) a lane inside a group of G = 2^LG lanes, and bits
+// [LK+LG, LK+LG+LW) a warp.  A layer whose highest flipped bit is a register
+// bit is a compare-exchange between two registers of the same thread; a lane
+// bit makes it one __shfl_xor_sync per element; a warp bit makes it one
+// shared-memory publish + read per element, double-buffered so that each such
+// layer costs a single __syncthreads.  With K = 32 and a warp per 1024-key
+// array, 40 of the 55 layers run in registers and 15 on the shuffle unit;
+// none touches shared memory.
+#pragma once
+#include <cstdint>
+#include <type_traits>
+
+#include "elem.cuh"
+
+namespace b200s {
+
+template <int I, int N, class F>
+__device__ __forceinline__ void sfor(F&& f) {
+    if constexpr (I < N) {
+        f(std::integral_constant<int, I>{});
+        sfor<I + 1, N>(f);
+    }
+}
+
+constexpr int hibit(unsigned x) {
+    int b = -1;
+    while (x) {
+        x >>= 1;
+        ++b;
+    }
+    return b;
+}
+
+template <int LK_, int LG_, int LW_>
+struct Shape {
+    static constexpr int LK = LK_, LG = LG_, LW = LW_;
+    static constexpr int K = 1 << LK;          // elements per thread
+    static constexpr int G = 1 << LG;          // lanes per array inside a warp
+    static constexpr int TPA = G << LW;        // threads per array
+    static constexpr int LOGW = LK + LG + LW;
+    static constexpr int W = 1 << LOGW;        // working tile length
+    static_assert(LG >= 0 && LG <= 5, "lane bits");
+    static_assert(LW == 0 || LG == 5, "an array spanning warps uses whole warps");
+};
+
+// One comparator layer with partner mask MASK (compile-time).
+template <class E, class S, unsigned MASK>
+__device__ __forceinline__ void layer(typename E::Reg (&v)[S::K], const int t,
+                                      typename E::Reg*& cur, typename E::Reg*& nxt) {
+    using R = typename E::Reg;
+    constexpr int HB = hibit(MASK);
+    constexpr unsigned RM = MASK & unsigned(S::K - 1);
+    constexpr unsigned TM = MASK >> S::LK;
+    if constexpr (HB < S::LK) {
+        sfor<0, S::K>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr int p = q ^ int(MASK);
+            if constexpr (q < p) E::cex(v[q], v[p]);
+        });
+    } else if constexpr (HB < S::LK + S::LG) {
+        const bool upper = (t >> (HB - S::LK)) & 1;
+        if constexpr (RM == 0) {
+            sfor<0, S::K>([&](auto qc) {
+                constexpr int q = decltype(qc)::value;
+                const R b = E::shfl(v[q], int(TM));
+                v[q] = E::pick(v[q], b, upper);
+            });
+        } else {
+            // Reflection across lanes: the partner of (lane, q) is
+            // (lane ^ TM, q ^ RM).  Exchange both registers of a pair before
+            // updating either.
+            sfor<0, S::K>([&](auto qc) {
+                constexpr int q = decltype(qc)::value;
+                constexpr int p = q ^ int(RM);
+                if constexpr (q < p) {
+                    const R bq = E::shfl(v[p], int(TM));
+                    const R bp = E::shfl(v[q], int(TM));
+                    v[q] = E::pick(v[q], bq, upper);
+                    v[p] = E::pick(v[p], bp, upper);
+                }
+            });
+        }
+    } else {
+        const bool upper = (t >> (HB - S::LK)) & 1;
+        // Striped publication: register q of every thread forms one row, so
+        // both the publish and the partner read are bank-conflict free.
+        sfor<0, S::K>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            cur[q * S::TPA + t] = v[q];
+        });
+        __syncthreads();
+        sfor<0, S::K>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            const R b = cur[(q ^ int(RM)) * S::TPA + (t ^ int(TM))];
+            v[q] = E::pick(v[q], b, upper);
+        });
+        R* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+    }
+}
+
+template <class E, class S, int ST>
+__device__ __forceinline__ void stage(typename E::Reg (&v)[S::K], const int t,
+                                      typename E::Reg*& cur, typename E::Reg*& nxt) {
+    layer<E, S, (2u << ST) - 1u>(v, t, cur, nxt);   // reflection, span 2^ST
+    sfor<0, ST>([&](auto jc) {
+        constexpr int j = ST - 1 - decltype(jc)::value;
+        layer<E, S, (1u << j)>(v, t, cur, nxt);       // merges 2^(ST-1) .. 1
+    });
+}
+
+// Sort the W-element tile held by the TPA threads of one array.
+template <class E, class S>
+__device__ __forceinline__ void network(typename E::Reg (&v)[S::K], const int t,
+                                        typename E::Reg*& cur, typename E::Reg*& nxt) {
+    sfor<0, S::LOGW>([&](auto sc) { stage<E, S, decltype(sc)::value>(v, t, cur, nxt); });
+}
+
+// ---- tile load / store --------------------------------------------------------
+// Thread t of an array owns elements [t*K, t*K+K).  Whole, 16-byte aligned
+// spans move as 128-bit accesses; a ragged tail or an unaligned array start
+// falls back to one access per element.  Elements at or beyond n are padding.
+template <class E, int K>
+__device__ __forceinline__ void load_tile(typename E::Reg (&v)[K], const typename E::Mem* src,
+                                          const int base, const int n) {
+    using M = typename E::Mem;
+    constexpr int BYTES = K * int(sizeof(M));
+    if constexpr (BYTES % 16 == 0) {
+        if (base + K <= n && (reinterpret_cast<uintptr_t>(src + base) & 15u) == 0) {
+            uint4 raw[BYTES / 16];
+            const uint4* p = reinterpret_cast<const uint4*>(src + base);
+#pragma unroll
+            for (int c = 0; c < BYTES / 16; ++c) raw[c] = __ldcs(p + c);
+            const M* m = reinterpret_cast<const M*>(raw);
+#pragma unroll
+            for (int q = 0; q < K; ++q) v[q] = E::from_mem(m[q], base + q);
+            return;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const int idx = base + q;
+        v[q] = idx < n ? E::from_mem(src[idx], idx) : E::pad();
+    }
+}
+
+template <class E, int K>
+__device__ __forceinline__ void store_tile(const typename E::Reg (&v)[K], typename E::Mem* dst,
+                                           const int base, const int n) {
+    using M = typename E::Mem;
+    constexpr int BYTES = K * int(sizeof(M));
+    if constexpr (BYTES % 16 == 0) {
+        if (base + K <= n && (reinterpret_cast<uintptr_t>(dst + base) & 15u) == 0) {
+            uint4 raw[BYTES / 16];
+            M* m = reinterpret_cast<M*>(raw);
+#pragma unroll
+            for (int q = 0; q < K; ++q) m[q] = E::to_mem(v[q]);
+            uint4* p = reinterpret_cast<uint4*>(dst + base);
+#pragma unroll
+            for (int c = 0; c < BYTES / 16; ++c) __stcs(p + c, raw[c]);
+            return;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const int idx = base + q;
+        if (idx < n) dst[idx] = E::to_mem(v[q]);
+    }
+}
+
+// ---- packed batch kernel ------------------------------------------------------
+// Packed layout of the reference's batched wrappers (bench.cu:355-393):
+// array a occupies [a*n, a*n + n).  Each group of TPA threads sorts one array;
+// a CTA holds CTA/TPA groups and strides over the batch.  The loop bound is
+// uniform across the CTA, so groups past the end sort padding and store
+// nothing, and every warp-wide shuffle and barrier sees all its threads.
+template <class E, class S, int CTA>
+__global__ void __launch_bounds__(CTA) k_sort_packed(const typename E::Mem* in,
+                                                     typename E::Mem* out, int n,
+                                                     long long arrays) {
+    using R = typename E::Reg;
+    static_assert(CTA % S::TPA == 0, "CTA holds whole arrays");
+    static_assert(S::LW == 0 || CTA == S::TPA, "a multi-warp array owns its CTA");
+    constexpr int APC = CTA / S::TPA;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* cur = reinterpret_cast<R*>(smem_raw);
+    R* nxt = cur + S::W;
+    const int slot = int(threadIdx.x) / S::TPA;
+    const int t = int(threadIdx.x) % S::TPA;
+    for (long long first = (long long)blockIdx.x * APC; first < arrays;
+         first += (long long)gridDim.x * APC) {
+        const long long a = first + slot;
+        const int na = a < arrays ? n : 0;
+        const long long off = (a < arrays ? a : 0) * (long long)n;
+        R v[S::K];
+        load_tile<E, S::K>(v, in + off, t * S::K, na);
+        network<E, S>(v, t, cur, nxt);
+        store_tile<E, S::K>(v, out + off, t * S::K, na);
+    }
+}
+
+}  // namespace b200s

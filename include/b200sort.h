@@ -1,0 +1,122 @@
+/*
+ * b200sort — batched small-array sort for NVIDIA B200 (sm_100a), C ABI.
+ *
+ * Drop-in for the one-CTA-per-array bitonic path of berenger-eu/cuda-sort.
+ * The reference exposes that path as header-only CUDA templates launched one
+ * CTA per array over a packed batch; this library exports the same operation
+ * as plain C entry points over caller-owned device buffers:
+ *
+ *   reference                                              this library
+ *   ---------------------------------------------------    ---------------------------
+ *   cusort_v6::Sort<T,W,Threads,...>(in, out, n)           b200s_sort_packed
+ *     cusort_v6.hpp:144-178, kernel cusort_v6.hpp:181-184
+ *   batched wrapper benchmarkSortV6Register<<<A,...>>>      b200s_sort_packed
+ *     (segment = data + blockIdx.x * n), bench.cu:389-393
+ *   cusort_experiment::Sort / Sort_1Block_v4_xor /          b200s_sort_packed
+ *     Sort_1Block_v5_static, cusort_experiments.hpp:366-419
+ *   Sort_1Block_gt32_d_extsm_v3 (cusort.hpp:1229-1231),     b200s_sort_packed
+ *     Sort_1Warp_SM_le32_d (cusort.hpp:574-575)
+ *   SortPartitionsAdaptive_outofplace over CSR partitions   b200s_sort_ragged / b200s_plan_*
+ *     (cusort.hpp:2309-2352; one launch, ragged lengths)
+ *   Batch::run host-to-device restore + launch              b200s_sort_packed_host
+ *     (bench.cu:320-352)
+ *
+ * Semantics shared with the reference:
+ *   - ascending by key; records (IntAndData, intanddata.hpp:9-52) compare by
+ *     key only and move with their payload;
+ *   - the default (unstable) mode applies the reference's comparator network
+ *     with its keep-own rule on ties, so record outputs, including the order
+ *     of equal keys, are identical to the reference's;
+ *   - in-place operation (d_in == d_out) is allowed, as bench.cu:392 uses it;
+ *   - the caller owns every buffer; the sort entry points allocate nothing.
+ * Differences: errors are returned as status codes instead of device asserts
+ * or exit() (cusort.hpp:240-245); every call takes a stream; lengths are not
+ * capped by the reference's 48 KB shared-memory rule (cusort.hpp:231-237).
+ *
+ * Streams are passed as `void*` holding a cudaStream_t (NULL = legacy default
+ * stream).  Entry points are safe to call from several host threads as long
+ * as each session/plan is used by one thread at a time.
+ */
+#ifndef B200SORT_H
+#define B200SORT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum b200s_status {
+    B200S_OK = 0,
+    B200S_ERR_INVALID_ARGUMENT = 1, /* null pointer, negative size, bad flag */
+    B200S_ERR_UNSUPPORTED = 2,      /* no compiled kernel covers this dtype/length/tile */
+    B200S_ERR_CUDA = 3,             /* a CUDA runtime call failed; see b200s_last_error() */
+    B200S_ERR_OUT_OF_MEMORY = 4,    /* a session/plan/server could not allocate */
+    B200S_ERR_TIMEOUT = 5,          /* a bounded wait gave up */
+    B200S_ERR_BUDGET = 6            /* request larger than the server's device-memory budget */
+} b200s_status;
+
+typedef enum b200s_dtype {
+    B200S_I32 = 0,     /* int32_t keys                                              */
+    B200S_I32_I32 = 1, /* {int32_t key; int32_t data;}  == IntAndData, 8 bytes      */
+    B200S_U64 = 2,     /* uint64_t keys                                             */
+    B200S_U64_I32 = 3  /* {uint64_t key; int32_t data; int32_t reserved;}, 16 bytes */
+} b200s_dtype;
+
+/* flags */
+#define B200S_STABLE 1u       /* ties keep input order (bit-exact std::stable_sort) */
+#define B200S_SORTED_CHECK 2u /* accepted for source compatibility with the reference's
+                                 `Sorted` switch; the output is identical either way   */
+
+/* A tile shape: how one array is laid over threads.  K = 2^log2_items
+ * elements per thread, 2^log2_lanes lanes per array inside a warp, and
+ * 2^log2_warps warps per array.  The working length is
+ * W = 2^(log2_items + log2_lanes + log2_warps) and must be >= n. */
+typedef struct b200s_tile {
+    int32_t log2_items;
+    int32_t log2_lanes;
+    int32_t log2_warps;
+    int32_t cta_threads; /* threads per CTA (output of the query functions) */
+} b200s_tile;
+
+const char* b200s_version(void);
+const char* b200s_status_string(b200s_status status);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* b200s_last_error(void);
+
+/* Largest array length the packed path handles for dtype/flags. */
+int32_t b200s_max_length(b200s_dtype dtype, uint32_t flags);
+
+/* Compiled tiles, for autotuning: index in [0, b200s_tile_count). */
+int32_t b200s_tile_count(b200s_dtype dtype, uint32_t flags);
+b200s_status b200s_tile_get(b200s_dtype dtype, uint32_t flags, int32_t index, b200s_tile* out);
+/* Tile the library uses for arrays of length n when the caller passes none. */
+b200s_status b200s_default_tile(b200s_dtype dtype, uint32_t flags, int32_t n, b200s_tile* out);
+/* Replace the default tile table from a CSV file (dtype,flags,log2_w,log2_items,
+ * log2_lanes,log2_warps per line; '#' comments).  Returns the number of rows
+ * applied in *applied. */
+b200s_status b200s_load_tile_table(const char* path, int32_t* applied);
+
+/* Sort `arrays` independent arrays of n elements each, packed back to back
+ * (array a at element offset a*n), from d_in into d_out (device pointers; may
+ * be equal).  tile == NULL uses the default tile for n. */
+b200s_status b200s_sort_packed(b200s_dtype dtype, const void* d_in, void* d_out, int32_t n,
+                               int64_t arrays, uint32_t flags, const b200s_tile* tile,
+                               void* stream);
+
+/* ---- host-buffer entry point (end to end) ------------------------------- */
+typedef struct b200s_session b200s_session;
+b200s_status b200s_session_create(b200s_session** out, int32_t device);
+b200s_status b200s_session_destroy(b200s_session* session);
+/* Same as b200s_sort_packed, on host buffers: the batch is copied to the
+ * device in chunks, sorted and copied back, with the copies of one chunk
+ * overlapping the sort of another.  Pinned host buffers give full PCIe
+ * bandwidth.  Returns after the output is in h_out. */
+b200s_status b200s_sort_packed_host(b200s_session* session, b200s_dtype dtype, const void* h_in,
+                                    void* h_out, int32_t n, int64_t arrays, uint32_t flags);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200SORT_H */

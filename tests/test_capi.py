@@ -1,0 +1,86 @@
+"""CPU checks of the C ABI: the library loads, exports every declared entry
+point, and rejects bad arguments before touching a GPU."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import b200sort as bs
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.join(ROOT, "include")))
+           if f.endswith(".h")]
+
+
+def _declared():
+    names = set()
+    for h in HEADERS:
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(b200s_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_every_declared_symbol_is_exported():
+    names = _declared()
+    assert "b200s_sort_packed" in names and len(names) >= 10
+    handle = ctypes.CDLL(bs.LIB_PATH)
+    missing = [n for n in names if not hasattr(handle, n)]
+    assert not missing, missing
+
+
+def test_version_and_status_strings():
+    assert "sm_100a" in bs.version()
+    for s in range(7):
+        assert bs.lib().b200s_status_string(s)
+
+
+@pytest.mark.parametrize("args,status", [
+    ((9, 16, 16, 10, 1, 0), bs.STATUS_NAMES and 1),     # unknown dtype
+    ((bs.I32, 16, 16, -1, 1, 0), 1),                     # negative n
+    ((bs.I32, 16, 16, 10, -1, 0), 1),                    # negative arrays
+    ((bs.I32, 16, 16, 10, 1, 0x80), 1),                  # unknown flag
+    ((bs.I32, 0, 16, 10, 1, 0), 1),                      # null input
+    ((bs.I32, 16, 0, 10, 1, 0), 1),                      # null output
+    ((bs.I32, 16, 16, 1 << 30, 1, 0), 2),                # longer than any tile
+    ((bs.I32, 0, 0, 0, 5, 0), 0),                        # empty arrays: nothing to do
+    ((bs.I32, 0, 0, 7, 0, 0), 0),                        # no arrays: nothing to do
+])
+def test_argument_checks_need_no_gpu(args, status):
+    dtype, pin, pout, n, arrays, flags = args
+    assert bs.sort_packed_status(dtype, pin, pout, n, arrays, flags) == status
+
+
+def test_explicit_tile_must_cover_n():
+    t = bs.default_tile(bs.I32, 100)
+    assert (1 << sum(t.as_tuple())) >= 100
+    short = bs.Tile(3, 0, 0, 0)
+    assert bs.sort_packed_status(bs.I32, 16, 16, 100, 1, 0, short) == 2
+    bogus = bs.Tile(9, 9, 9, 0)
+    assert bs.sort_packed_status(bs.I32, 16, 16, 10, 1, 0, bogus) == 2
+
+
+def test_tile_registry_covers_every_length_up_to_the_maximum():
+    for dtype in (bs.I32, bs.I32_I32, bs.U64, bs.U64_I32):
+        for flags in (0, bs.STABLE):
+            top = bs.max_length(dtype, flags)
+            assert top >= 4096
+            assert len(bs.tiles(dtype, flags)) >= 8
+            for n in [1, 2, 3, 31, 32, 33, 1000, 1024, 1025, top // 2 + 1, top]:
+                t = bs.default_tile(dtype, n, flags)
+                w = 1 << sum(t.as_tuple())
+                assert w >= n and t.cta_threads % 32 == 0
+
+
+def test_tile_table_file_round_trip(tmp_path):
+    t = bs.tiles(bs.I32)[0]
+    p = tmp_path / "table.csv"
+    p.write_text("# dtype,flags,log2_w,log2_items,log2_lanes,log2_warps\n0,0,%d,%d,%d,%d\n"
+                 % (sum(t.as_tuple()), t.log2_items, t.log2_lanes, t.log2_warps))
+    assert bs.load_tile_table(str(p)) == 1
+    bad = tmp_path / "bad.csv"
+    bad.write_text("0,0,3,9,9,9\n")
+    with pytest.raises(bs.B200SortError):
+        bs.load_tile_table(str(bad))
