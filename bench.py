@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--preroll", type=float, default=1.5,
+                    help="seconds of untimed sorting before the timed region, so clocks settle")
     return ap.parse_args()
 
 
@@ -262,7 +264,7 @@ def main():
         pass
     sampler.start()
     # Pre-roll so that the clocks settle under load before the timed region.
-    t_end = time.perf_counter() + 1.5
+    t_end = time.perf_counter() + args.preroll
     i = 0
     while time.perf_counter() < t_end:
         for _ in range(50):

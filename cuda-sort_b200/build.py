@@ -14,6 +14,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libb200sort.so")
+BASELINES = os.path.join(HERE, "baselines")
+CUB_LIB = os.path.join(HERE, "libb200sort_cub.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -61,9 +63,22 @@ def build(verbose=False, extra=None, jobs=None):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+    build_cub_baseline()
     if verbose:
-        print("built", LIB)
+        print("built", LIB, CUB_LIB)
     return LIB
+
+
+def build_cub_baseline():
+    """The CUB BlockMergeSort baseline library (timed beside the product, never linked into it)."""
+    src = os.path.join(BASELINES, "cub_block_merge.cu")
+    if os.path.exists(CUB_LIB) and os.path.getmtime(CUB_LIB) >= os.path.getmtime(src):
+        return CUB_LIB
+    cmd = [NVCC] + ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", src, "-o", CUB_LIB]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("CUB baseline build failed:\n" + r.stdout + r.stderr)
+    return CUB_LIB
 
 
 if __name__ == "__main__":

@@ -70,7 +70,8 @@ namespace {
 constexpr int kMaxLog2W = 20;
 
 struct DefaultTable {
-    int pick[4][2][kMaxLog2W + 1];
+    int pick[4][2][kMaxLog2W + 1];        // registry index, -1 if none
+    int persistent[4][2][kMaxLog2W + 1];  // launch form for that row
 };
 
 std::mutex g_table_mutex;
@@ -96,6 +97,7 @@ DefaultTable build_defaults() {
                     }
                 }
                 t.pick[d][s][w] = best;
+                t.persistent[d][s][w] = 0;
             }
     return t;
 }
@@ -107,11 +109,14 @@ DefaultTable& table() {
 
 // Entry for arrays of length n: the tabled tile for the smallest compiled
 // working length >= n.
-int lookup_default(int dtype, int stable, long long n) {
+int lookup_default(int dtype, int stable, long long n, int* persistent) {
     std::lock_guard<std::mutex> lock(g_table_mutex);
     const DefaultTable& t = table();
     for (int w = std::max(0, ceil_log2(n)); w <= kMaxLog2W; ++w)
-        if (t.pick[dtype][stable][w] >= 0) return t.pick[dtype][stable][w];
+        if (t.pick[dtype][stable][w] >= 0) {
+            *persistent = t.persistent[dtype][stable][w];
+            return t.pick[dtype][stable][w];
+        }
     return -1;
 }
 
@@ -126,11 +131,12 @@ int lookup_tile(int dtype, int stable, const b200s_tile& tile) {
     return -1;
 }
 
-void fill_tile(const KernelEntry& e, b200s_tile* out) {
+void fill_tile(const KernelEntry& e, int persistent, b200s_tile* out) {
     out->log2_items = e.lk;
     out->log2_lanes = e.lg;
     out->log2_warps = e.lw;
     out->cta_threads = e.cta;
+    out->persistent = persistent;
 }
 
 bool valid_dtype(int d) { return d >= 0 && d <= 3; }
@@ -138,20 +144,24 @@ bool valid_dtype(int d) { return d >= 0 && d <= 3; }
 }  // namespace
 
 // Launch the packed kernel of registry entry `idx`.
-b200s_status launch_packed(int idx, const void* in, void* out, int n, long long arrays,
-                           cudaStream_t st) {
+b200s_status launch_packed(int idx, int persistent, const void* in, void* out, int n,
+                           long long arrays, cudaStream_t st) {
     const KernelEntry& e = registry()[size_t(idx)];
     long long grid = (arrays + e.apc - 1) / e.apc;
     grid = std::min<long long>(grid, 0x7fffffffLL);
-    cudaError_t err = e.launch(in, out, n, arrays, grid, st);
+    cudaError_t err = persistent ? e.launch_pf(in, out, n, arrays, grid, st)
+                                 : e.launch(in, out, n, arrays, grid, st);
     if (err != cudaSuccess) return cuda_error(err, "sort kernel launch");
     return B200S_OK;
 }
 
-int select_entry(int dtype, uint32_t flags, long long n, const b200s_tile* tile, b200s_status* st) {
+int select_entry(int dtype, uint32_t flags, long long n, const b200s_tile* tile, b200s_status* st,
+                 int* persistent) {
     const int stable = effective_stable(dtype, flags);
     int idx;
+    *persistent = 0;
     if (tile) {
+        *persistent = tile->persistent ? 1 : 0;
         idx = lookup_tile(dtype, stable, *tile);
         if (idx < 0) {
             *st = set_error(B200S_ERR_UNSUPPORTED, "no compiled kernel for the requested tile");
@@ -162,7 +172,7 @@ int select_entry(int dtype, uint32_t flags, long long n, const b200s_tile* tile,
             return -1;
         }
     } else {
-        idx = lookup_default(dtype, stable, n);
+        idx = lookup_default(dtype, stable, n, persistent);
         if (idx < 0) {
             *st = set_error(B200S_ERR_UNSUPPORTED, "array length exceeds the largest compiled tile");
             return -1;
@@ -221,7 +231,7 @@ b200s_status b200s_tile_get(b200s_dtype dtype, uint32_t flags, int32_t index, b2
     for (const KernelEntry& e : registry()) {
         if (e.dtype != dtype || e.stable != stable) continue;
         if (c++ == index) {
-            fill_tile(e, out);
+            fill_tile(e, 0, out);
             return B200S_OK;
         }
     }
@@ -232,9 +242,10 @@ b200s_status b200s_default_tile(b200s_dtype dtype, uint32_t flags, int32_t n, b2
     if (!valid_dtype(dtype) || !out || n < 0)
         return set_error(B200S_ERR_INVALID_ARGUMENT, "b200s_default_tile: bad argument");
     b200s_status st;
-    const int idx = select_entry(dtype, flags, std::max(1, n), nullptr, &st);
+    int persistent = 0;
+    const int idx = select_entry(dtype, flags, std::max(1, n), nullptr, &st, &persistent);
     if (idx < 0) return st;
-    fill_tile(registry()[size_t(idx)], out);
+    fill_tile(registry()[size_t(idx)], persistent, out);
     return B200S_OK;
 }
 
@@ -244,7 +255,7 @@ b200s_status b200s_load_tile_table(const char* path, int32_t* applied) {
     if (!f) return set_error(B200S_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path);
     std::string line;
     int rows = 0, lineno = 0;
-    std::vector<std::array<int, 3>> updates;  // dtype*2+stable, log2w, index
+    std::vector<std::array<int, 4>> updates;  // dtype*2+stable, log2w, index, persistent
     while (std::getline(f, line)) {
         ++lineno;
         const size_t hash = line.find('#');
@@ -252,26 +263,30 @@ b200s_status b200s_load_tile_table(const char* path, int32_t* applied) {
         if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
         std::replace(line.begin(), line.end(), ',', ' ');
         std::istringstream ss(line);
-        int d, fl, w, lk, lg, lw;
+        int d, fl, w, lk, lg, lw, pers = 0;
         if (!(ss >> d >> fl >> w >> lk >> lg >> lw))
             return set_error(B200S_ERR_INVALID_ARGUMENT,
-                             "tile table line " + std::to_string(lineno) + ": expected 6 integers");
+                             "tile table line " + std::to_string(lineno) + ": expected 6 or 7 integers");
+        if (!(ss >> pers)) pers = 0;
         if (!valid_dtype(d) || w < 0 || w > 20)
             return set_error(B200S_ERR_INVALID_ARGUMENT,
                              "tile table line " + std::to_string(lineno) + ": bad dtype or log2_w");
         const int stable = effective_stable(d, uint32_t(fl));
-        const b200s_tile tile{lk, lg, lw, 0};
+        const b200s_tile tile{lk, lg, lw, 0, 0};
         const int idx = lookup_tile(d, stable, tile);
         if (idx < 0 || registry()[size_t(idx)].log2w < w)
             return set_error(B200S_ERR_UNSUPPORTED,
                              "tile table line " + std::to_string(lineno) + ": tile not compiled or too short");
-        updates.push_back({d * 2 + stable, w, idx});
+        updates.push_back({d * 2 + stable, w, idx, pers ? 1 : 0});
         ++rows;
     }
     {
         std::lock_guard<std::mutex> lock(g_table_mutex);
         DefaultTable& t = table();
-        for (const auto& u : updates) t.pick[u[0] / 2][u[0] % 2][u[1]] = u[2];
+        for (const auto& u : updates) {
+            t.pick[u[0] / 2][u[0] % 2][u[1]] = u[2];
+            t.persistent[u[0] / 2][u[0] % 2][u[1]] = u[3];
+        }
     }
     if (applied) *applied = rows;
     clear_error();
@@ -288,9 +303,10 @@ b200s_status b200s_sort_packed(b200s_dtype dtype, const void* d_in, void* d_out,
     if (n == 0 || arrays == 0) return B200S_OK;
     if (!d_in || !d_out) return set_error(B200S_ERR_INVALID_ARGUMENT, "null buffer");
     b200s_status st;
-    const int idx = select_entry(dtype, flags, n, tile, &st);
+    int persistent = 0;
+    const int idx = select_entry(dtype, flags, n, tile, &st, &persistent);
     if (idx < 0) return st;
-    return launch_packed(idx, d_in, d_out, n, arrays, static_cast<cudaStream_t>(stream));
+    return launch_packed(idx, persistent, d_in, d_out, n, arrays, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"
@@ -361,7 +377,8 @@ b200s_status b200s_sort_packed_host(b200s_session* s, b200s_dtype dtype, const v
     if (n == 0 || arrays == 0) return B200S_OK;
     if (!h_in || !h_out) return set_error(B200S_ERR_INVALID_ARGUMENT, "null buffer");
     b200s_status st;
-    const int idx = select_entry(dtype, flags, n, nullptr, &st);
+    int persistent = 0;
+    const int idx = select_entry(dtype, flags, n, nullptr, &st, &persistent);
     if (idx < 0) return st;
     cudaError_t e = cudaSetDevice(s->device);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
@@ -397,7 +414,7 @@ b200s_status b200s_sort_packed_host(b200s_session* s, b200s_dtype dtype, const v
         e = cudaMemcpyAsync(s->dbuf[k], src + size_t(first) * array_bytes, bytes,
                             cudaMemcpyHostToDevice, stream);
         if (e != cudaSuccess) return cuda_error(e, "host-to-device copy");
-        st = launch_packed(idx, s->dbuf[k], s->dbuf[k], n, count, stream);
+        st = launch_packed(idx, persistent, s->dbuf[k], s->dbuf[k], n, count, stream);
         if (st != B200S_OK) return st;
         e = cudaMemcpyAsync(dst + size_t(first) * array_bytes, s->dbuf[k], bytes,
                             cudaMemcpyDeviceToHost, stream);

@@ -78,12 +78,40 @@ struct Packed {
             ids, count);
         return cudaGetLastError();
     }
+    // Persistent launch: as many CTAs as fit at once (cached per device), never
+    // more than the batch needs.
+    static cudaError_t launch_pf(const void* in, void* out, int n, long long arrays, long long grid,
+                                 cudaStream_t st) {
+        auto fn = k_sort_packed_pf<E, S, CTA>;
+        cudaError_t e = prepare(reinterpret_cast<const void*>(fn));
+        if (e != cudaSuccess) return e;
+        static std::atomic<int> resident[64];
+        int dev = 0;
+        e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        int cap = resident[dev & 63].load(std::memory_order_relaxed);
+        if (cap == 0) {
+            int per_sm = 0, sms = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, CTA, SMEM);
+            if (e != cudaSuccess) return e;
+            e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (e != cudaSuccess) return e;
+            cap = per_sm * sms;
+            if (cap <= 0) return cudaErrorInvalidConfiguration;
+            resident[dev & 63].store(cap, std::memory_order_relaxed);
+        }
+        const long long g = grid < cap ? grid : cap;
+        fn<<<dim3(unsigned(g)), dim3(CTA), SMEM, st>>>(
+            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), n, arrays);
+        return cudaGetLastError();
+    }
     static cudaError_t attrs(cudaFuncAttributes* a) {
         return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(k_sort_packed<E, S, CTA>));
     }
     static KernelEntry entry(int dtype) {
-        return KernelEntry{dtype,  E::kStable ? 1 : 0, LK,      LG,     LW,         CTA,
-                           S::LOGW, SMEM,              CTA / S::TPA, &launch, &attrs, &launch_list};
+        return KernelEntry{dtype,   E::kStable ? 1 : 0, LK,     LG,         LW,
+                           CTA,     S::LOGW,            SMEM,   CTA / S::TPA, &launch,
+                           &attrs,  &launch_list,       &launch_pf};
     }
 };
 

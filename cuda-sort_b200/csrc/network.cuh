@@ -214,4 +214,39 @@ __global__ void __launch_bounds__(CTA) k_sort_packed(const typename E::Mem* in,
     }
 }
 
+// Persistent form: the grid is sized to the resident capacity and each group
+// walks the batch with a stride of the whole grid, loading the next array's
+// tile into registers before sorting the current one, so that the global
+// loads of one array overlap the comparator layers of the previous one.
+template <class E, class S, int CTA>
+__global__ void __launch_bounds__(CTA) k_sort_packed_pf(const typename E::Mem* in,
+                                                        typename E::Mem* out, int n,
+                                                        long long arrays) {
+    using R = typename E::Reg;
+    constexpr int APC = CTA / S::TPA;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* cur = reinterpret_cast<R*>(smem_raw);
+    R* nxt = cur + S::W;
+    const int slot = int(threadIdx.x) / S::TPA;
+    const int t = int(threadIdx.x) % S::TPA;
+    const long long stride = (long long)gridDim.x * APC;
+    long long first = (long long)blockIdx.x * APC;
+    if (first >= arrays) return;  // uniform across the CTA
+    R v[S::K];
+    {
+        const long long a = first + slot;
+        load_tile<E, S::K>(v, in + (a < arrays ? a : 0) * (long long)n, t * S::K, a < arrays ? n : 0);
+    }
+    for (; first < arrays; first += stride) {
+        const long long a = first + slot;
+        const long long an = a + stride;
+        R w[S::K];
+        load_tile<E, S::K>(w, in + (an < arrays ? an : 0) * (long long)n, t * S::K, an < arrays ? n : 0);
+        network<E, S>(v, t, cur, nxt);
+        if (a < arrays) store_tile<E, S::K>(v, out + a * (long long)n, t * S::K, n);
+#pragma unroll
+        for (int q = 0; q < S::K; ++q) v[q] = w[q];
+    }
+}
+
 }  // namespace b200s

@@ -26,9 +26,10 @@ struct KernelEntry {
     int log2w;        // working length exponent
     size_t smem;      // dynamic shared memory bytes
     int apc;          // arrays per CTA
-    PackedLaunch launch;
+    PackedLaunch launch;      // one group per array, grid covers the batch
     AttrQuery attrs;
     ListLaunch launch_list;
+    PackedLaunch launch_pf;   // persistent grid, next-array prefetch
 };
 
 void register_i32(std::vector<KernelEntry>& out);

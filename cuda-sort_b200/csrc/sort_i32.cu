@@ -25,6 +25,10 @@ void register_i32(std::vector<KernelEntry>& o) {
     o.push_back(Packed<ElemI32, 4, 5, 0>::entry(D));
     o.push_back(Packed<ElemI32, 4, 5, 1>::entry(D));
     o.push_back(Packed<ElemI32, 4, 5, 2>::entry(D));
+    // K = 64: ten shuffle layers instead of fifteen for a 1024-key array.
+    o.push_back(Packed<ElemI32, 6, 3, 0>::entry(D));
+    o.push_back(Packed<ElemI32, 6, 4, 0>::entry(D));
+    o.push_back(Packed<ElemI32, 6, 5, 0>::entry(D));
 }
 
 }  // namespace b200s

@@ -77,6 +77,8 @@ typedef struct b200s_tile {
     int32_t log2_lanes;
     int32_t log2_warps;
     int32_t cta_threads; /* threads per CTA (output of the query functions) */
+    int32_t persistent;  /* 0: one launch slot per array group; 1: grid sized to the
+                            resident capacity, each group prefetching its next array */
 } b200s_tile;
 
 const char* b200s_version(void);
@@ -92,9 +94,9 @@ int32_t b200s_tile_count(b200s_dtype dtype, uint32_t flags);
 b200s_status b200s_tile_get(b200s_dtype dtype, uint32_t flags, int32_t index, b200s_tile* out);
 /* Tile the library uses for arrays of length n when the caller passes none. */
 b200s_status b200s_default_tile(b200s_dtype dtype, uint32_t flags, int32_t n, b200s_tile* out);
-/* Replace the default tile table from a CSV file (dtype,flags,log2_w,log2_items,
- * log2_lanes,log2_warps per line; '#' comments).  Returns the number of rows
- * applied in *applied. */
+/* Replace rows of the default tile table from a CSV file (dtype,flags,log2_w,
+ * log2_items,log2_lanes,log2_warps,persistent per line; '#' comments).  Returns
+ * the number of rows applied in *applied. */
 b200s_status b200s_load_tile_table(const char* path, int32_t* applied);
 
 /* Sort `arrays` independent arrays of n elements each, packed back to back

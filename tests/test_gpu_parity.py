@@ -76,13 +76,14 @@ def test_distributions(dtype, dist):
 @pytest.mark.parametrize("dtype", ALL)
 def test_every_compiled_tile_gives_the_same_output(dtype):
     for flags in (0, bs.STABLE):
-        for tile in bs.tiles(dtype, flags):
-            w = 1 << sum(tile.as_tuple())
-            for n in sorted({max(1, w // 2 + 1), w}):
-                arrays = 300 if w <= 256 else 4
-                data = workloads.make_packed(dtype, n, arrays, "distinct16", seed=w + n, extremes=True)
-                got = gpu_sort(dtype, data, n, arrays, flags, tile=tile)
-                check(dtype, flags, data, n, arrays, got)
+        for base in bs.tiles(dtype, flags):
+            w = 1 << sum(base.as_tuple())
+            for tile in (base, base.with_persistent()):
+                for n in sorted({max(1, w // 2 + 1), w}):
+                    arrays = 300 if w <= 256 else 4
+                    data = workloads.make_packed(dtype, n, arrays, "distinct16", seed=w + n, extremes=True)
+                    got = gpu_sort(dtype, data, n, arrays, flags, tile=tile)
+                    check(dtype, flags, data, n, arrays, got)
 
 
 @pytest.mark.parametrize("dtype", ALL)
@@ -108,8 +109,24 @@ def test_reference_known_answer_inputs():
 def test_headline_batch_4096_by_1024_int32():
     n, arrays = 1024, 4096
     data = workloads.make_packed(bs.I32, n, arrays, "uniform", seed=2024)
+    want = np.sort(data.reshape(arrays, n), axis=1)
     got = gpu_sort(bs.I32, data, n, arrays)
-    assert np.array_equal(got.reshape(arrays, n), np.sort(data.reshape(arrays, n), axis=1))
+    assert np.array_equal(got.reshape(arrays, n), want)
+    # every tile that covers n, in both launch forms (the persistent form walks
+    # several arrays per group here)
+    for base in bs.tiles(bs.I32):
+        if (1 << sum(base.as_tuple())) < n:
+            continue
+        for tile in (base, base.with_persistent()):
+            got = gpu_sort(bs.I32, data, n, arrays, tile=tile)
+            assert np.array_equal(got.reshape(arrays, n), want), repr(tile)
+
+
+def test_persistent_form_over_many_arrays_per_group():
+    for dtype, n, arrays in ((bs.I32_I32, 2048, 3000), (bs.I32_I32, 100, 200000), (bs.U64_I32, 4096, 700)):
+        data = workloads.make_packed(dtype, n, arrays, "distinct16", seed=arrays, extremes=True)
+        tile = bs.default_tile(dtype, n).with_persistent()
+        check(dtype, 0, data, n, arrays, gpu_sort(dtype, data, n, arrays, tile=tile))
 
 
 @pytest.mark.parametrize("n", [32, 129, 256, 1000, 2048, 4096])
