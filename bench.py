@@ -9,7 +9,14 @@ range (one batch per rank; ranks are independent replicas, weak scaling).
 
 One step = one sort of one batch already resident in HBM (out of place).
 Steps rotate over enough input/output sets that every step reads inputs
-evicted from the 126 MB L2.  Rank 0 prints one JSON line.
+evicted from the 126 MB L2 (batches larger than L2 use one set).  Rank 0
+prints one JSON line.
+
+Workloads: int32_4096x1024 (default), records_n{32,129,256,1000,2048,4096}
+(IntAndData records, 4194304 per batch), ragged_200000 (200000 CSR arrays,
+lengths log-uniform in [1, 8192], records; the persistent bucketed launch
+replayed from its CUDA graph, with the plain per-length launches timed
+beside it).
 
 --impl reference times the reference's own CPU path on this host (one
 std::sort per array over all host threads, compiled from the reference's
@@ -40,11 +47,12 @@ L2_BYTES = 126 * 1024 * 1024
 FALLBACK_HBM_GBS = 6650.0
 
 WORKLOADS = {
-    "int32_4096x1024": dict(dtype=bs.I32, n=1024, arrays=4096, dist="uniform", flags=0),
-    "records_n4096": dict(dtype=bs.I32_I32, n=4096, arrays=1024, dist="uniform", flags=0),
-    "records_n1000": dict(dtype=bs.I32_I32, n=1000, arrays=4194, dist="uniform", flags=0),
-    "records_n32": dict(dtype=bs.I32_I32, n=32, arrays=131072, dist="uniform", flags=0),
+    "int32_4096x1024": dict(kind="packed", dtype=bs.I32, n=1024, arrays=4096, dist="uniform", flags=0),
+    "ragged_200000": dict(kind="ragged", dtype=bs.I32_I32, arrays=200000, max_len=8192, dist="uniform", flags=0),
 }
+for _n in (32, 129, 256, 1000, 2048, 4096):
+    WORKLOADS["records_n%d" % _n] = dict(kind="packed", dtype=bs.I32_I32, n=_n, arrays=4194304 // _n,
+                                         dist="uniform", flags=0)
 DTYPE_NAMES = {bs.I32: "int32", bs.I32_I32: "int32+int32", bs.U64: "uint64", bs.U64_I32: "uint64+int32"}
 
 
@@ -67,9 +75,9 @@ def peaks():
     try:
         with open(path) as f:
             p = json.load(f)
-        return float(p["hbm_gbs"]), "measured"
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
     except (OSError, KeyError, ValueError):
-        return FALLBACK_HBM_GBS, "fallback"
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
 
 
 def traffic_for(workload):
@@ -139,46 +147,70 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_reference_sort(data, n, arrays, threads):
-    """The reference's own per-array std::sort (oracle/_ref), or the oracle port."""
+# ---- CPU baseline: the reference's own std::sort per array (oracle/_ref) ------------
+
+def _cpu_runner(data, wl, threads, off=None):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import cpu_oracle as orc
 
-    if orc.ref_cpu_available() and data.dtype in (bs.NP_DTYPES[bs.I32], bs.NP_DTYPES[bs.I32_I32]):
-        code = 0 if data.dtype == bs.NP_DTYPES[bs.I32] else 1
-        return (lambda buf: orc.ref_cpu_sort_inplace(code, buf, n, arrays, threads)), "reference"
-
-    def port(buf):
-        dtype = {v: k for k, v in bs.NP_DTYPES.items()}[buf.dtype]
-        buf[:] = orc.sort_packed(dtype, buf, n, arrays, orc.MODE_STD, threads)
+    dtype = wl["dtype"]
+    if orc.ref_cpu_available() and dtype in (bs.I32, bs.I32_I32):
+        code = 0 if dtype == bs.I32 else 1
+        if off is None:
+            return (lambda buf: orc.ref_cpu_sort_inplace(code, buf, wl["n"], wl["arrays"], threads)), "reference"
+        return (lambda buf: orc.ref_cpu_sort_ragged_inplace(code, buf, off, threads)), "reference"
+    if off is None:
+        def port(buf):
+            buf[:] = orc.sort_packed(dtype, buf, wl["n"], wl["arrays"], orc.MODE_STD, threads)
+    else:
+        def port(buf):
+            buf[:] = orc.sort_ragged(dtype, buf, off, orc.MODE_STD, threads)
     return port, "port"
 
 
-def time_cpu(data, n, arrays, threads, budget_s=8.0, min_reps=2, max_reps=50):
-    run, kind = cpu_reference_sort(data, n, arrays, threads)
-    times = []
-    t_total = 0.0
-    while len(times) < max_reps and (len(times) < min_reps or t_total < budget_s):
+def time_cpu(data, wl, threads, off=None, budget_s=8.0, min_reps=2, max_reps=50):
+    run, kind = _cpu_runner(data, wl, threads, off)
+    times, total = [], 0.0
+    while len(times) < max_reps and (len(times) < min_reps or total < budget_s):
         buf = data.copy()
         t0 = time.perf_counter()
         run(buf)
         dt = time.perf_counter() - t0
         times.append(dt)
-        t_total += dt
+        total += dt
     return statistics.median(times), kind, len(times)
+
+
+def make_input(wl, seed):
+    if wl["kind"] == "packed":
+        return workloads.make_packed(wl["dtype"], wl["n"], wl["arrays"], wl["dist"], seed=seed), None
+    lengths = workloads.ragged_lengths(wl["arrays"], max_len=wl["max_len"], seed=seed)
+    return workloads.make_ragged(wl["dtype"], lengths, wl["dist"], seed=seed)
+
+
+def config_of(args, wl, data):
+    c = {"workload": args.workload, "kind": wl["kind"], "arrays_per_gpu": wl["arrays"],
+         "key_dtype": DTYPE_NAMES[wl["dtype"]], "distribution": wl["dist"],
+         "stable": bool(wl["flags"] & bs.STABLE), "parallelism": "replicas (arrays are independent)",
+         "keys_per_gpu": int(len(data))}
+    if wl["kind"] == "packed":
+        c["n"] = wl["n"]
+        c["l2"] = "inputs rotate over sets larger than L2 (126 MB)"
+    else:
+        c["lengths"] = "log-uniform in [1, %d], CSR int32 offsets" % wl["max_len"]
+        c["l2"] = "input %.2f GB, larger than L2" % (data.nbytes / 1e9)
+    return c
 
 
 def reference_arm(args, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    n, arrays, dtype = wl["n"], wl["arrays"], wl["dtype"]
-    data = workloads.make_packed(dtype, n, arrays, wl["dist"], seed=1234)
+    data, off = make_input(wl, 1234)
     threads = os.cpu_count() or 1
-    run, kind = cpu_reference_sort(data, n, arrays, threads)
+    run, kind = _cpu_runner(data, wl, threads, off)
     for _ in range(args.warmup):
-        buf = data.copy()
-        run(buf)
+        run(data.copy())
     total = 0.0
     for _ in range(args.steps):
         buf = data.copy()
@@ -186,26 +218,247 @@ def reference_arm(args, wl):
         run(buf)
         total += time.perf_counter() - t0
     sec = total / max(1, args.steps)
-    value = n * arrays / sec
+    value = len(data) / sec
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": DTYPE_NAMES[dtype], "data": "synthetic",
-        "config": config_of(args, wl),
+        "scaling": "weak", "vs_baseline": None, "dtype": DTYPE_NAMES[wl["dtype"]], "data": "synthetic",
+        "config": config_of(args, wl, data),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                         "sample": "the full batch (%d arrays x %d) per step, std::sort per array over %d "
-                                   "host threads" % (arrays, n, threads)},
+                         "sample": "the full batch (%d arrays, %d keys) per step, std::sort per array over %d "
+                                   "host threads" % (wl["arrays"], len(data), threads)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
 
 
-def config_of(args, wl):
-    return {"workload": args.workload, "arrays_per_gpu": wl["arrays"], "n": wl["n"],
-            "key_dtype": DTYPE_NAMES[wl["dtype"]], "distribution": wl["dist"],
-            "stable": bool(wl["flags"] & bs.STABLE), "parallelism": "replicas",
-            "l2": "inputs rotate over sets larger than L2 (126 MB)"}
+# ---- GPU arm ---------------------------------------------------------------------
+
+class Ctx:
+    def __init__(self):
+        import torch
+        import torch.distributed as dist
+
+        self.torch, self.dist = torch, dist
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(self.local)
+        self.dev = torch.device("cuda", self.local)
+        if self.world > 1:
+            import datetime
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=self.dev)
+        self.stream = torch.cuda.current_stream(self.dev)
+        self.sh = self.stream.cuda_stream
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max_over_ranks(self, x):
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sync(self):
+        self.torch.cuda.synchronize(self.dev)
+
+    def event_time(self, step, count):
+        """Device time of `count` back-to-back steps, between a barrier and a sync on both sides."""
+        torch = self.torch
+        self.barrier()
+        self.sync()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(self.stream)
+        for j in range(count):
+            step(j)
+        ev1.record(self.stream)
+        self.sync()
+        self.barrier()
+        return self.max_over_ranks(ev0.elapsed_time(ev1))
+
+
+def timed_region(ctx, step, args):
+    for i in range(max(3, args.warmup)):
+        step(i)
+    ctx.sync()
+    sampler = ClockSampler(None)
+    try:
+        uuid = str(ctx.torch.cuda.get_device_properties(ctx.dev).uuid)
+        sampler = ClockSampler(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+    except Exception:
+        pass
+    sampler.start()
+    t_end = time.perf_counter() + args.preroll
+    i = 0
+    while time.perf_counter() < t_end:
+        for _ in range(10):
+            step(i)
+            i += 1
+        ctx.sync()
+    ms_total = ctx.event_time(step, args.steps)
+    sampler.stop()
+    return ms_total / args.steps, sampler.summary()
+
+
+def verify_ragged(dtype, data, off, got):
+    """Size-independent checks: sorted within every array, per-array key sums
+    equal, and (records) every payload is the position of an equal key of the
+    same array, each position used once."""
+    keys_in = data if dtype in (bs.I32, bs.U64) else data["key"]
+    keys = got if dtype in (bs.I32, bs.U64) else got["key"]
+    starts = off[:-1]
+    nonempty = off[1:] > starts
+    boundary = np.zeros(len(keys), dtype=bool)
+    boundary[starts[nonempty]] = True
+    ok = bool(np.all((keys[1:] >= keys[:-1]) | boundary[1:]))
+    s_in = np.add.reduceat(keys_in.astype(np.int64), starts[nonempty]) if nonempty.any() else 0
+    s_out = np.add.reduceat(keys.astype(np.int64), starts[nonempty]) if nonempty.any() else 0
+    ok = ok and bool(np.array_equal(s_in, s_out))
+    if dtype in (bs.I32_I32, bs.U64_I32):
+        pos = got["data"].astype(np.int64)
+        arr = np.repeat(np.arange(len(off) - 1), np.diff(off))
+        ok = ok and bool(np.all((pos >= off[arr]) & (pos < off[arr + 1])))
+        ok = ok and bool(np.array_equal(keys_in[pos], keys))
+        ok = ok and bool(np.all(np.bincount(pos, minlength=len(keys)) == 1))
+    return ok
+
+
+def run_gpu(args, wl):
+    ctx = Ctx()
+    torch = ctx.torch
+    dtype, flags = wl["dtype"], wl["flags"]
+    eb = bs.ELEM_BYTES[dtype]
+    data, off = make_input(wl, 1234 + ctx.rank)
+    total_keys = len(data)
+    batch_bytes = data.nbytes
+    host = torch.from_numpy(data.view(np.uint8).copy())
+    extra = {}
+
+    if wl["kind"] == "packed":
+        n, arrays = wl["n"], wl["arrays"]
+        sets = max(2, math.ceil(2 * L2_BYTES / batch_bytes) + 1) if batch_bytes < 2 * L2_BYTES else 1
+        d_in = [host.to(ctx.dev) for _ in range(sets)]
+        d_out = [torch.empty_like(d_in[0]) for _ in range(sets)]
+
+        def step(i):
+            k = i % sets
+            bs.sort_packed(dtype, d_in[k].data_ptr(), d_out[k].data_ptr(), n, arrays, flags, None, ctx.sh)
+
+        ms_step, clocks = timed_region(ctx, step, args)
+        got = d_out[(args.steps - 1) % sets].cpu().numpy().view(bs.NP_DTYPES[dtype])
+        keys_in = data if dtype in (bs.I32, bs.U64) else data["key"]
+        keys_out = got if dtype in (bs.I32, bs.U64) else got["key"]
+        verified = bool(np.array_equal(keys_out.reshape(arrays, n), np.sort(keys_in.reshape(arrays, n), axis=1)))
+        kernel = "k_sort_packed"
+        launches = args.steps
+    else:
+        arrays = wl["arrays"]
+        d_in = host.to(ctx.dev)
+        d_out = torch.empty_like(d_in)
+        d_off = torch.from_numpy(off.astype(np.int32)).to(ctx.dev)
+        plan = bs.Plan(dtype, arrays, flags, ctx.local)
+
+        def step(i):
+            plan.sort(d_in.data_ptr(), d_out.data_ptr(), d_off.data_ptr(), arrays, ctx.sh)
+
+        ms_step, clocks = timed_region(ctx, step, args)
+        got = d_out.cpu().numpy().view(bs.NP_DTYPES[dtype])
+        verified = verify_ragged(dtype, data, off, got) and plan.too_long(ctx.sh) == 0
+        kernel = "k_sort_ragged"
+        launches = 3 * args.steps   # bin count, bin scatter, sort (one graph per step)
+        # the plain per-length launches on the same input
+        plain_launches = plan.prepare_plain(off.astype(np.int32))
+        d_out.zero_()
+
+        def plain(i):
+            plan.sort_plain(d_in.data_ptr(), d_out.data_ptr(), d_off.data_ptr(), ctx.sh)
+
+        for i in range(2):
+            plain(i)
+        psteps = max(2, min(args.steps, 5))
+        ms_plain = ctx.event_time(plain, psteps) / psteps
+        verified = verified and verify_ragged(dtype, data, off, d_out.cpu().numpy().view(bs.NP_DTYPES[dtype]))
+        extra["baselines"] = {"plain_per_length": {
+            "ms_per_step": ms_plain, "value": total_keys * ctx.world / (ms_plain * 1e-3), "unit": UNIT,
+            "launches_per_step": plain_launches,
+            "persistent_graph_speedup": ms_plain / ms_step}}
+
+    value = total_keys * ctx.world / (ms_step * 1e-3)
+    hbm, peak_src = peaks()
+    algo_bytes = 2 * batch_bytes
+    achieved = algo_bytes / (ms_step * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "peak_source": peak_src, "traffic": traffic_for(args.workload),
+                "algorithmic_bytes_per_launch": algo_bytes, "kernel": kernel, "launch_us": ms_step * 1e3}
+
+    e2e = None
+    if not args.no_e2e:
+        pin_in = host.pin_memory()
+        pin_out = torch.empty_like(pin_in).pin_memory()
+        esteps = max(3, min(args.steps, 30 if wl["kind"] == "packed" else 5))
+        if wl["kind"] == "packed":
+            with bs.Session(ctx.local) as sess:
+                def e2e_step():
+                    sess.sort_host(dtype, pin_in.data_ptr(), pin_out.data_ptr(), wl["n"], wl["arrays"], flags)
+                e2e_step()
+                ctx.barrier()
+                t0 = time.perf_counter()
+                for _ in range(esteps):
+                    e2e_step()
+                dt = time.perf_counter() - t0
+            path = "b200s_sort_packed_host (pinned host buffers, chunked copy/sort overlap)"
+            h2d = batch_bytes
+        else:
+            pin_off = torch.from_numpy(off.astype(np.int32)).pin_memory()
+
+            def e2e_step():
+                d_in.copy_(pin_in, non_blocking=True)
+                d_off.copy_(pin_off, non_blocking=True)
+                plan.sort(d_in.data_ptr(), d_out.data_ptr(), d_off.data_ptr(), wl["arrays"], ctx.sh)
+                pin_out.copy_(d_out, non_blocking=True)
+                ctx.sync()
+            e2e_step()
+            ctx.barrier()
+            t0 = time.perf_counter()
+            for _ in range(esteps):
+                e2e_step()
+            dt = time.perf_counter() - t0
+            path = "pinned copies + b200s_sort_ragged (plan graph) + pinned copy back"
+            h2d = batch_bytes + pin_off.numel() * 4
+        ctx.barrier()
+        dt = ctx.max_over_ranks(dt)
+        e2e = {"value": total_keys * ctx.world * esteps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": batch_bytes, "steps": esteps, "path": path}
+        out = pin_out.numpy().view(bs.NP_DTYPES[dtype])
+        verified = verified and bool(np.array_equal(out["key"] if dtype in (bs.I32_I32, bs.U64_I32) else out,
+                                                    got["key"] if dtype in (bs.I32_I32, bs.U64_I32) else got))
+
+    cpu = None
+    if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sec, kind, reps = time_cpu(data, wl, threads, off)
+        cpu = {"value": total_keys / sec, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": "the full batch (%d arrays, %d keys), %d repetitions, std::sort per array"
+                         % (wl["arrays"], total_keys, reps)}
+
+    if ctx.world > 1:
+        ctx.dist.destroy_process_group()
+    if ctx.rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ctx.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": DTYPE_NAMES[dtype], "data": "synthetic",
+        "config": config_of(args, wl, data), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": launches, "clocks": clocks, "verified": verified, "library": bs.version(),
+    }
+    line.update(extra)
+    print(json.dumps(line))
+    return 0 if verified else 1
 
 
 def main():
@@ -213,144 +466,7 @@ def main():
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         return reference_arm(args, wl)
-
-    import torch
-    import torch.distributed as dist
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    dtype, n, arrays, flags = wl["dtype"], wl["n"], wl["arrays"], wl["flags"]
-    eb = bs.ELEM_BYTES[dtype]
-    batch_bytes = n * arrays * eb
-    data = workloads.make_packed(dtype, n, arrays, wl["dist"], seed=1234 + rank)
-    sets = max(2, math.ceil(2 * L2_BYTES / batch_bytes) + 1)
-    host = torch.from_numpy(data.view(np.uint8).copy())
-    d_in = [host.to(dev) for _ in range(sets)]
-    d_out = [torch.empty_like(d_in[0]) for _ in range(sets)]
-    stream = torch.cuda.current_stream(dev)
-    sh = stream.cuda_stream
-
-    def step(i):
-        k = i % sets
-        bs.sort_packed(dtype, d_in[k].data_ptr(), d_out[k].data_ptr(), n, arrays, flags, None, sh)
-
-    for i in range(max(3, args.warmup)):
-        step(i)
-    torch.cuda.synchronize(dev)
-
-    sampler = ClockSampler(None)
-    try:
-        uuid = str(torch.cuda.get_device_properties(dev).uuid)
-        sampler = ClockSampler(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
-    except Exception:
-        pass
-    sampler.start()
-    # Pre-roll so that the clocks settle under load before the timed region.
-    t_end = time.perf_counter() + args.preroll
-    i = 0
-    while time.perf_counter() < t_end:
-        for _ in range(50):
-            step(i)
-            i += 1
-        torch.cuda.synchronize(dev)
-
-    barrier()
-    torch.cuda.synchronize(dev)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for j in range(args.steps):
-        step(j)
-    ev1.record(stream)
-    torch.cuda.synchronize(dev)
-    barrier()
-    ms_total = ev0.elapsed_time(ev1)
-    sampler.stop()
-    ms_total = max_over_ranks(ms_total)
-    ms_step = ms_total / args.steps
-
-    # correctness of the last timed output (outside timing)
-    k = (args.steps - 1) % sets
-    got = d_out[k].cpu().numpy().view(bs.NP_DTYPES[dtype])
-    if dtype in (bs.I32, bs.U64):
-        verified = bool(np.array_equal(got.reshape(arrays, n), np.sort(data.reshape(arrays, n), axis=1)))
-    else:
-        verified = bool(np.array_equal(got["key"].reshape(arrays, n),
-                                       np.sort(data["key"].reshape(arrays, n), axis=1)))
-
-    keys_per_step = n * arrays
-    value = keys_per_step * world / (ms_step * 1e-3)
-    hbm, peak_src = peaks()
-    algo_bytes = 2 * batch_bytes
-    achieved = algo_bytes / (ms_step * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
-                else "fallback 6.65 TB/s",
-                "traffic": traffic_for(args.workload), "algorithmic_bytes_per_launch": algo_bytes,
-                "kernel": "k_sort_packed", "launch_us": ms_step * 1e3}
-
-    e2e = None
-    if not args.no_e2e:
-        pin_in = host.pin_memory()
-        pin_out = torch.empty_like(pin_in).pin_memory()
-        esteps = max(3, min(args.steps, 30))
-        with bs.Session(local) as sess:
-            for _ in range(2):
-                sess.sort_host(dtype, pin_in.data_ptr(), pin_out.data_ptr(), n, arrays, flags)
-            barrier()
-            t0 = time.perf_counter()
-            for _ in range(esteps):
-                sess.sort_host(dtype, pin_in.data_ptr(), pin_out.data_ptr(), n, arrays, flags)
-            dt = time.perf_counter() - t0
-            barrier()
-        dt = max_over_ranks(dt)
-        e2e = {"value": keys_per_step * world * esteps / dt, "unit": UNIT, "h2d_bytes_per_step": batch_bytes,
-               "d2h_bytes_per_step": batch_bytes, "steps": esteps,
-               "path": "b200s_sort_packed_host (pinned host buffers, chunked copy/sort overlap)"}
-        out = pin_out.numpy().view(bs.NP_DTYPES[dtype])
-        if dtype in (bs.I32, bs.U64):
-            verified = verified and bool(np.array_equal(out, got))
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        sec, kind, reps = time_cpu(data, n, arrays, threads)
-        cpu = {"value": keys_per_step / sec, "unit": UNIT, "cores": threads, "kind": kind,
-               "sample": "the full batch (%d arrays x %d), %d repetitions, std::sort per array"
-                         % (arrays, n, reps)}
-
-    if world > 1:
-        dist.destroy_process_group()
-    if rank != 0:
-        return 0
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": DTYPE_NAMES[dtype], "data": "synthetic",
-        "config": config_of(args, wl), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-        "gpu_launches": args.steps, "clocks": sampler.summary(), "verified": verified,
-        "library": bs.version(),
-    }
-    print(json.dumps(line))
-    return 0 if verified else 1
+    return run_gpu(args, wl)
 
 
 if __name__ == "__main__":

@@ -20,6 +20,7 @@ I32, I32_I32, U64, U64_I32 = 0, 1, 2, 3
 DTYPES = {"i32": I32, "i32_i32": I32_I32, "u64": U64, "u64_i32": U64_I32}
 STABLE = 1
 SORTED_CHECK = 2
+PLAN_NO_GRAPH = 0x100
 ELEM_BYTES = {I32: 4, I32_I32: 8, U64: 8, U64_I32: 16}
 
 # numpy views of the memory layouts
@@ -72,6 +73,17 @@ _SIGNATURES = {
     "b200s_sort_packed": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                          ctypes.c_int64, ctypes.c_uint32, ctypes.POINTER(Tile),
                                          ctypes.c_void_p]),
+    "b200s_plan_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_uint32,
+                                         ctypes.c_int64, ctypes.c_int32]),
+    "b200s_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "b200s_ragged_max_length": (ctypes.c_int32, [ctypes.c_int, ctypes.c_uint32]),
+    "b200s_sort_ragged": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_int64, ctypes.c_void_p]),
+    "b200s_plan_too_long": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    "b200s_plan_prepare_plain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]),
+    "b200s_sort_ragged_plain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_void_p]),
+    "b200s_plan_plain_launches": (ctypes.c_int32, [ctypes.c_void_p]),
     "b200s_session_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32]),
     "b200s_session_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "b200s_sort_packed_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
@@ -165,6 +177,54 @@ class Session:
     def close(self):
         if self._h:
             lib().b200s_session_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ragged_max_length(dtype, flags=0):
+    return lib().b200s_ragged_max_length(dtype, flags)
+
+
+class Plan:
+    """A ragged-batch plan: scratch for max_arrays arrays and a captured CUDA graph."""
+
+    def __init__(self, dtype, max_arrays, flags=0, device=0):
+        self.dtype = dtype
+        self._h = ctypes.c_void_p()
+        check(lib().b200s_plan_create(ctypes.byref(self._h), dtype, flags, max_arrays, device))
+
+    def sort(self, d_in, d_out, d_offsets, arrays, stream=0):
+        return check(lib().b200s_sort_ragged(self._h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out),
+                                             ctypes.c_void_p(d_offsets), arrays, ctypes.c_void_p(stream)))
+
+    def too_long(self, stream=0):
+        c = ctypes.c_int64(0)
+        check(lib().b200s_plan_too_long(self._h, ctypes.c_void_p(stream), ctypes.byref(c)))
+        return c.value
+
+    def prepare_plain(self, h_offsets_int32):
+        off = np.ascontiguousarray(h_offsets_int32, dtype=np.int32)
+        check(lib().b200s_plan_prepare_plain(self._h, ctypes.c_void_p(off.ctypes.data), len(off) - 1))
+        return lib().b200s_plan_plain_launches(self._h)
+
+    def sort_plain(self, d_in, d_out, d_offsets, stream=0):
+        return check(lib().b200s_sort_ragged_plain(self._h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out),
+                                                   ctypes.c_void_p(d_offsets), ctypes.c_void_p(stream)))
+
+    def close(self):
+        if self._h:
+            lib().b200s_plan_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __enter__(self):

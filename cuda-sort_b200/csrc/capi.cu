@@ -143,6 +143,12 @@ bool valid_dtype(int d) { return d >= 0 && d <= 3; }
 
 }  // namespace
 
+int lookup_default_entry(int dtype, int stable, long long n, int* persistent) {
+    return lookup_default(dtype, stable, n, persistent);
+}
+
+void set_ragged_family(int dtype, int stable, int log2w, int family);
+
 // Launch the packed kernel of registry entry `idx`.
 b200s_status launch_packed(int idx, int persistent, const void* in, void* out, int n,
                            long long arrays, cudaStream_t st) {
@@ -256,6 +262,7 @@ b200s_status b200s_load_tile_table(const char* path, int32_t* applied) {
     std::string line;
     int rows = 0, lineno = 0;
     std::vector<std::array<int, 4>> updates;  // dtype*2+stable, log2w, index, persistent
+    std::vector<std::array<int, 4>> ragged_rows;  // dtype, stable, log2w, family
     while (std::getline(f, line)) {
         ++lineno;
         const size_t hash = line.find('#');
@@ -263,6 +270,18 @@ b200s_status b200s_load_tile_table(const char* path, int32_t* applied) {
         if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
         std::replace(line.begin(), line.end(), ',', ' ');
         std::istringstream ss(line);
+        const size_t first = line.find_first_not_of(" \t");
+        if (line[first] == 'r') {
+            // ragged row: r dtype flags log2_w family
+            std::string tag;
+            int d, fl, w, fam;
+            if (!(ss >> tag >> d >> fl >> w >> fam) || !valid_dtype(d) || w < 3 || w > 18 || fam < 0 || fam > 1)
+                return set_error(B200S_ERR_INVALID_ARGUMENT,
+                                 "tile table line " + std::to_string(lineno) + ": bad ragged row");
+            ragged_rows.push_back({d, effective_stable(d, uint32_t(fl)), w, fam});
+            ++rows;
+            continue;
+        }
         int d, fl, w, lk, lg, lw, pers = 0;
         if (!(ss >> d >> fl >> w >> lk >> lg >> lw))
             return set_error(B200S_ERR_INVALID_ARGUMENT,
@@ -288,6 +307,7 @@ b200s_status b200s_load_tile_table(const char* path, int32_t* applied) {
             t.persistent[u[0] / 2][u[0] % 2][u[1]] = u[3];
         }
     }
+    for (const auto& r : ragged_rows) set_ragged_family(r[0], r[1], r[2], r[3]);
     if (applied) *applied = rows;
     clear_error();
     return B200S_OK;

@@ -5,39 +5,10 @@
 #include <atomic>
 
 #include "network.cuh"
+#include "ragged.cuh"
 #include "registry.h"
 
 namespace b200s {
-
-// Ragged-list kernel: CTA-group g sorts array ids[g] whose elements start at
-// start[id] and number len[id].  Used by the per-bucket launches of a plan.
-template <class E, class S, int CTA>
-__global__ void __launch_bounds__(CTA) k_sort_list(const typename E::Mem* in, typename E::Mem* out,
-                                                   const long long* start, const int* len,
-                                                   const int* ids, long long count) {
-    using R = typename E::Reg;
-    constexpr int APC = CTA / S::TPA;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* cur = reinterpret_cast<R*>(smem_raw);
-    R* nxt = cur + S::W;
-    const int slot = int(threadIdx.x) / S::TPA;
-    const int t = int(threadIdx.x) % S::TPA;
-    for (long long first = (long long)blockIdx.x * APC; first < count;
-         first += (long long)gridDim.x * APC) {
-        const long long g = first + slot;
-        int na = 0;
-        long long off = 0;
-        if (g < count) {
-            const int id = ids[g];
-            na = len[id];
-            off = start[id];
-        }
-        R v[S::K];
-        load_tile<E, S::K>(v, in + off, t * S::K, na);
-        network<E, S>(v, t, cur, nxt);
-        store_tile<E, S::K>(v, out + off, t * S::K, na);
-    }
-}
 
 template <class E, int LK, int LG, int LW>
 struct Packed {
@@ -45,9 +16,11 @@ struct Packed {
     static constexpr int CTA = LW > 0 ? S::TPA : (S::TPA >= 128 ? S::TPA : 128);
     static constexpr size_t SMEM = LW > 0 ? 2 * size_t(S::W) * sizeof(typename E::Reg) : 0;
 
+    // The opt-in above 48 KB is per kernel and per device; WHICH keeps one
+    // record per kernel of this tile (0 packed, 1 list, 2 persistent).
+    template <int WHICH>
     static cudaError_t prepare(const void* fn) {
         if (SMEM <= 48 * 1024) return cudaSuccess;
-        // The opt-in above 48 KB is per device; remember which devices have it.
         static std::atomic<unsigned long long> done{0};
         int dev = 0;
         cudaError_t e = cudaGetDevice(&dev);
@@ -61,21 +34,20 @@ struct Packed {
     static cudaError_t launch(const void* in, void* out, int n, long long arrays, long long grid,
                               cudaStream_t st) {
         auto fn = k_sort_packed<E, S, CTA>;
-        cudaError_t e = prepare(reinterpret_cast<const void*>(fn));
+        cudaError_t e = prepare<0>(reinterpret_cast<const void*>(fn));
         if (e != cudaSuccess) return e;
         fn<<<dim3(unsigned(grid)), dim3(CTA), SMEM, st>>>(
             static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), n, arrays);
         return cudaGetLastError();
     }
-    static cudaError_t launch_list(const void* in, void* out, const long long* start, const int* len,
-                                   const int* ids, long long count, long long grid,
+    static cudaError_t launch_list(const void* in, void* out, const int* off, const int* ids, int count,
                                    cudaStream_t st) {
-        auto fn = k_sort_list<E, S, CTA>;
-        cudaError_t e = prepare(reinterpret_cast<const void*>(fn));
+        auto fn = k_sort_idlist<E, S, CTA>;
+        cudaError_t e = prepare<1>(reinterpret_cast<const void*>(fn));
         if (e != cudaSuccess) return e;
+        const int grid = (count + CTA / S::TPA - 1) / (CTA / S::TPA);
         fn<<<dim3(unsigned(grid)), dim3(CTA), SMEM, st>>>(
-            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), start, len,
-            ids, count);
+            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), off, ids, count);
         return cudaGetLastError();
     }
     // Persistent launch: as many CTAs as fit at once (cached per device), never
@@ -83,7 +55,7 @@ struct Packed {
     static cudaError_t launch_pf(const void* in, void* out, int n, long long arrays, long long grid,
                                  cudaStream_t st) {
         auto fn = k_sort_packed_pf<E, S, CTA>;
-        cudaError_t e = prepare(reinterpret_cast<const void*>(fn));
+        cudaError_t e = prepare<2>(reinterpret_cast<const void*>(fn));
         if (e != cudaSuccess) return e;
         static std::atomic<int> resident[64];
         int dev = 0;
@@ -112,6 +84,38 @@ struct Packed {
         return KernelEntry{dtype,   E::kStable ? 1 : 0, LK,     LG,         LW,
                            CTA,     S::LOGW,            SMEM,   CTA / S::TPA, &launch,
                            &attrs,  &launch_list,       &launch_pf};
+    }
+};
+
+// The persistent ragged kernel of element type E.
+template <class E, int CTA, int NB, int LKA, int LKB>
+struct Ragged {
+    static constexpr size_t SMEM = ragged_smem<E, CTA, NB, LKA, LKB>();
+    static cudaError_t launch(const void* in, void* out, const int* off, const int* ids, RaggedCtl* ctl,
+                              unsigned family_mask, int grid, cudaStream_t st) {
+        auto fn = k_sort_ragged<E, CTA, NB, LKA, LKB>;
+        if (SMEM > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM));
+            if (e != cudaSuccess) return e;
+        }
+        fn<<<dim3(unsigned(grid)), dim3(CTA), SMEM, st>>>(static_cast<const typename E::Mem*>(in),
+                                                          static_cast<typename E::Mem*>(out), off, ids, ctl,
+                                                          family_mask);
+        return cudaGetLastError();
+    }
+    static int resident_per_sm() {
+        auto fn = k_sort_ragged<E, CTA, NB, LKA, LKB>;
+        if (SMEM > 48 * 1024 &&
+            cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(SMEM)) != cudaSuccess)
+            return 0;
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, CTA, SMEM) != cudaSuccess) return 0;
+        return per_sm;
+    }
+    static RaggedEntry entry(int dtype) {
+        return RaggedEntry{dtype, E::kStable ? 1 : 0, CTA, NB, LKA, LKB, SMEM, &launch, &resident_per_sm};
     }
 };
 

@@ -36,6 +36,20 @@ __device__ __forceinline__ void sfor(F&& f) {
     }
 }
 
+// Barrier over the threads that share one array's shared-memory tile: the
+// whole CTA when an array owns its CTA, or a named barrier when several
+// multi-warp teams share a CTA (ids 1..15; id 0 is __syncthreads).
+struct CtaBarrier {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct TeamBarrier {
+    int id;
+    int threads;
+    __device__ __forceinline__ void operator()() const {
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+    }
+};
+
 constexpr int hibit(unsigned x) {
     int b = -1;
     while (x) {
@@ -58,9 +72,9 @@ struct Shape {
 };
 
 // One comparator layer with partner mask MASK (compile-time).
-template <class E, class S, unsigned MASK>
+template <class E, class S, unsigned MASK, class Bar>
 __device__ __forceinline__ void layer(typename E::Reg (&v)[S::K], const int t,
-                                      typename E::Reg*& cur, typename E::Reg*& nxt) {
+                                      typename E::Reg*& cur, typename E::Reg*& nxt, const Bar& bar) {
     using R = typename E::Reg;
     constexpr int HB = hibit(MASK);
     constexpr unsigned RM = MASK & unsigned(S::K - 1);
@@ -102,7 +116,7 @@ __device__ __forceinline__ void layer(typename E::Reg (&v)[S::K], const int t,
             constexpr int q = decltype(qc)::value;
             cur[q * S::TPA + t] = v[q];
         });
-        __syncthreads();
+        bar();
         sfor<0, S::K>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
             const R b = cur[(q ^ int(RM)) * S::TPA + (t ^ int(TM))];
@@ -114,21 +128,22 @@ __device__ __forceinline__ void layer(typename E::Reg (&v)[S::K], const int t,
     }
 }
 
-template <class E, class S, int ST>
+template <class E, class S, int ST, class Bar>
 __device__ __forceinline__ void stage(typename E::Reg (&v)[S::K], const int t,
-                                      typename E::Reg*& cur, typename E::Reg*& nxt) {
-    layer<E, S, (2u << ST) - 1u>(v, t, cur, nxt);   // reflection, span 2^ST
+                                      typename E::Reg*& cur, typename E::Reg*& nxt, const Bar& bar) {
+    layer<E, S, (2u << ST) - 1u>(v, t, cur, nxt, bar);   // reflection, span 2^ST
     sfor<0, ST>([&](auto jc) {
         constexpr int j = ST - 1 - decltype(jc)::value;
-        layer<E, S, (1u << j)>(v, t, cur, nxt);       // merges 2^(ST-1) .. 1
+        layer<E, S, (1u << j)>(v, t, cur, nxt, bar);       // merges 2^(ST-1) .. 1
     });
 }
 
 // Sort the W-element tile held by the TPA threads of one array.
-template <class E, class S>
+template <class E, class S, class Bar = CtaBarrier>
 __device__ __forceinline__ void network(typename E::Reg (&v)[S::K], const int t,
-                                        typename E::Reg*& cur, typename E::Reg*& nxt) {
-    sfor<0, S::LOGW>([&](auto sc) { stage<E, S, decltype(sc)::value>(v, t, cur, nxt); });
+                                        typename E::Reg*& cur, typename E::Reg*& nxt,
+                                        const Bar& bar = Bar()) {
+    sfor<0, S::LOGW>([&](auto sc) { stage<E, S, decltype(sc)::value>(v, t, cur, nxt, bar); });
 }
 
 // ---- tile load / store --------------------------------------------------------

@@ -1,0 +1,289 @@
+// Ragged-batch plans: scratch, the persistent bucketed launch, its CUDA
+// graph, and the plain per-length launches it is compared with.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "b200sort.h"
+#define B200S_DEFINE_BIN_KERNELS
+#include "ragged.cuh"
+#include "registry.h"
+
+namespace b200s {
+
+b200s_status set_error(b200s_status s, const std::string& msg);
+b200s_status cuda_error(cudaError_t e, const char* what);
+int effective_stable(int dtype, uint32_t flags);
+int ceil_log2(long long n);
+int lookup_default_entry(int dtype, int stable, long long n, int* persistent);
+b200s_status launch_packed(int idx, int persistent, const void* in, void* out, int n, long long arrays,
+                           cudaStream_t st);
+
+const std::vector<RaggedEntry>& ragged_registry() {
+    static std::vector<RaggedEntry> all = [] {
+        std::vector<RaggedEntry> v;
+        register_ragged_i32(v);
+        register_ragged_rec(v);
+        register_ragged_u64(v);
+        return v;
+    }();
+    return all;
+}
+
+namespace {
+
+std::mutex g_mask_mutex;
+unsigned g_family_mask[4][2] = {};
+
+const RaggedEntry* find_ragged(int dtype, int stable) {
+    for (const RaggedEntry& e : ragged_registry())
+        if (e.dtype == dtype && e.stable == stable) return &e;
+    return nullptr;
+}
+
+}  // namespace
+
+void set_ragged_family(int dtype, int stable, int log2w, int family) {
+    std::lock_guard<std::mutex> lock(g_mask_mutex);
+    const int b = log2w - kRaggedLmin;
+    if (b < 0 || b >= kMaxBuckets) return;
+    if (family) g_family_mask[dtype][stable] |= 1u << b;
+    else g_family_mask[dtype][stable] &= ~(1u << b);
+}
+
+unsigned ragged_family_mask(int dtype, int stable) {
+    std::lock_guard<std::mutex> lock(g_mask_mutex);
+    return g_family_mask[dtype][stable];
+}
+
+}  // namespace b200s
+
+using namespace b200s;
+
+struct b200s_plan {
+    int device = 0;
+    int dtype = 0;
+    int stable = 0;
+    uint32_t flags = 0;
+    long long max_arrays = 0;
+    const RaggedEntry* rk = nullptr;
+    unsigned family_mask = 0;
+    int grid = 0;       // persistent CTAs
+    int bin_grid = 0;   // CTAs of the binning kernels
+    void* scratch = nullptr;
+    RaggedCtl* ctl = nullptr;
+    int* ids = nullptr;
+    cudaStream_t capture = nullptr;
+    // the graph of the last (in, out, offsets, arrays)
+    cudaGraphExec_t exec = nullptr;
+    const void* g_in = nullptr;
+    void* g_out = nullptr;
+    const int* g_off = nullptr;
+    long long g_arrays = -1;
+    // plain per-length launches: ids grouped by exact length on the host
+    int* plain_ids = nullptr;
+    struct Group {
+        int n, first, count, entry, persistent;
+    };
+    std::vector<Group> groups;
+};
+
+namespace {
+
+b200s_status record_sequence(b200s_plan* p, const void* in, void* out, const int* off, int arrays,
+                             cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(p->ctl, 0, sizeof(RaggedCtl), st);
+    if (e != cudaSuccess) return cuda_error(e, "ragged control reset");
+    const int bin_threads = 256;
+    const int bin_grid = std::max(1, std::min(p->bin_grid, (arrays + bin_threads - 1) / bin_threads));
+    k_bin_count<<<bin_grid, bin_threads, 0, st>>>(off, arrays, p->ctl, p->rk->nb);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "bin count launch");
+    k_bin_scatter<<<bin_grid, bin_threads, 0, st>>>(off, arrays, p->ctl, p->ids, p->rk->nb);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "bin scatter launch");
+    e = p->rk->launch(in, out, off, p->ids, p->ctl, p->family_mask, p->grid, st);
+    if (e != cudaSuccess) return cuda_error(e, "ragged sort launch");
+    return B200S_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t b200s_ragged_max_length(b200s_dtype dtype, uint32_t flags) {
+    if (dtype < 0 || dtype > 3) return 0;
+    for (const RaggedEntry& e : ragged_registry())
+        if (e.dtype == dtype && e.stable == effective_stable(dtype, flags))
+            return int32_t(1) << (kRaggedLmin + e.nb - 1);
+    return 0;
+}
+
+b200s_status b200s_plan_create(b200s_plan** out, b200s_dtype dtype, uint32_t flags, int64_t max_arrays,
+                               int32_t device) {
+    if (!out) return set_error(B200S_ERR_INVALID_ARGUMENT, "null plan pointer");
+    *out = nullptr;
+    if (dtype < 0 || dtype > 3) return set_error(B200S_ERR_INVALID_ARGUMENT, "unknown dtype");
+    if (max_arrays < 0 || max_arrays > 0x7ffffffeLL)
+        return set_error(B200S_ERR_INVALID_ARGUMENT, "max_arrays out of range");
+    if (flags & ~(B200S_STABLE | B200S_SORTED_CHECK | B200S_PLAN_NO_GRAPH))
+        return set_error(B200S_ERR_INVALID_ARGUMENT, "unknown flag bits");
+    const int stable = effective_stable(dtype, flags);
+    const RaggedEntry* rk = find_ragged(dtype, stable);
+    if (!rk) return set_error(B200S_ERR_UNSUPPORTED, "no ragged kernel for this dtype");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    int sms = 0;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+        return cuda_error(e, "multiprocessor count");
+    const int per_sm = rk->resident_per_sm();
+    if (per_sm <= 0) return set_error(B200S_ERR_CUDA, "ragged kernel does not fit on this device");
+    auto* p = new b200s_plan();
+    p->device = device;
+    p->dtype = dtype;
+    p->stable = stable;
+    p->flags = flags;
+    p->max_arrays = max_arrays;
+    p->rk = rk;
+    p->family_mask = ragged_family_mask(dtype, stable);
+    p->grid = sms * per_sm;
+    p->bin_grid = sms * 4;
+    const size_t ids_bytes = size_t(std::max<long long>(1, max_arrays)) * sizeof(int);
+    e = cudaMalloc(&p->scratch, sizeof(RaggedCtl) + 2 * ids_bytes);
+    if (e != cudaSuccess) {
+        delete p;
+        return cuda_error(e, "plan scratch allocation");
+    }
+    p->ctl = static_cast<RaggedCtl*>(p->scratch);
+    p->ids = reinterpret_cast<int*>(static_cast<char*>(p->scratch) + sizeof(RaggedCtl));
+    p->plain_ids = p->ids + std::max<long long>(1, max_arrays);
+    e = cudaStreamCreateWithFlags(&p->capture, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cudaFree(p->scratch);
+        delete p;
+        return cuda_error(e, "capture stream");
+    }
+    *out = p;
+    return B200S_OK;
+}
+
+b200s_status b200s_plan_destroy(b200s_plan* p) {
+    if (!p) return B200S_OK;
+    cudaSetDevice(p->device);
+    if (p->capture) cudaStreamSynchronize(p->capture);
+    cudaDeviceSynchronize();
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->capture) cudaStreamDestroy(p->capture);
+    if (p->scratch) cudaFree(p->scratch);
+    delete p;
+    return B200S_OK;
+}
+
+b200s_status b200s_sort_ragged(b200s_plan* p, const void* d_in, void* d_out, const int32_t* d_offsets,
+                               int64_t arrays, void* stream) {
+    if (!p) return set_error(B200S_ERR_INVALID_ARGUMENT, "null plan");
+    if (arrays < 0 || arrays > p->max_arrays)
+        return set_error(B200S_ERR_INVALID_ARGUMENT, "arrays exceeds the plan's max_arrays");
+    if (arrays == 0) return B200S_OK;
+    if (!d_in || !d_out || !d_offsets) return set_error(B200S_ERR_INVALID_ARGUMENT, "null buffer");
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (p->flags & B200S_PLAN_NO_GRAPH) return record_sequence(p, d_in, d_out, d_offsets, int(arrays), st);
+    if (!p->exec || p->g_in != d_in || p->g_out != d_out || p->g_off != d_offsets || p->g_arrays != arrays) {
+        if (p->exec) {
+            // the previous graph may still run on another stream
+            cudaDeviceSynchronize();
+            cudaGraphExecDestroy(p->exec);
+            p->exec = nullptr;
+        }
+        e = cudaStreamBeginCapture(p->capture, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_error(e, "begin capture");
+        b200s_status st_rec = record_sequence(p, d_in, d_out, d_offsets, int(arrays), p->capture);
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamEndCapture(p->capture, &graph);
+        if (st_rec != B200S_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st_rec;
+        }
+        if (e != cudaSuccess) return cuda_error(e, "end capture");
+        e = cudaGraphInstantiate(&p->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            p->exec = nullptr;
+            return cuda_error(e, "graph instantiate");
+        }
+        p->g_in = d_in;
+        p->g_out = d_out;
+        p->g_off = d_offsets;
+        p->g_arrays = arrays;
+    }
+    e = cudaGraphLaunch(p->exec, st);
+    if (e != cudaSuccess) return cuda_error(e, "graph launch");
+    return B200S_OK;
+}
+
+b200s_status b200s_plan_too_long(b200s_plan* p, void* stream, int64_t* count) {
+    if (!p || !count) return set_error(B200S_ERR_INVALID_ARGUMENT, "null argument");
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    int v = 0;
+    e = cudaMemcpyAsync(&v, &p->ctl->too_long, sizeof(int), cudaMemcpyDeviceToHost,
+                        static_cast<cudaStream_t>(stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_error(e, "read ragged status");
+    *count = v;
+    return B200S_OK;
+}
+
+b200s_status b200s_plan_prepare_plain(b200s_plan* p, const int32_t* h_offsets, int64_t arrays) {
+    if (!p || (!h_offsets && arrays > 0)) return set_error(B200S_ERR_INVALID_ARGUMENT, "null argument");
+    if (arrays < 0 || arrays > p->max_arrays)
+        return set_error(B200S_ERR_INVALID_ARGUMENT, "arrays exceeds the plan's max_arrays");
+    // Counting sort of array ids by exact length.
+    int top = 0;
+    for (int64_t a = 0; a < arrays; ++a) {
+        const int n = h_offsets[a + 1] - h_offsets[a];
+        if (n < 0) return set_error(B200S_ERR_INVALID_ARGUMENT, "offsets decrease");
+        top = std::max(top, n);
+    }
+    std::vector<int> start(size_t(top) + 2, 0);
+    for (int64_t a = 0; a < arrays; ++a) ++start[size_t(h_offsets[a + 1] - h_offsets[a]) + 1];
+    for (size_t i = 1; i < start.size(); ++i) start[i] += start[i - 1];
+    std::vector<int> ids(size_t(std::max<int64_t>(arrays, 1)));
+    std::vector<int> cursor(start.begin(), start.end() - 1);
+    for (int64_t a = 0; a < arrays; ++a) ids[size_t(cursor[size_t(h_offsets[a + 1] - h_offsets[a])]++)] = int(a);
+    p->groups.clear();
+    for (int n = 1; n <= top; ++n) {
+        const int c = start[size_t(n) + 1] - start[size_t(n)];
+        if (!c) continue;
+        int persistent = 0;
+        const int entry = lookup_default_entry(p->dtype, p->stable, n, &persistent);
+        if (entry < 0) return set_error(B200S_ERR_UNSUPPORTED, "array longer than the largest tile");
+        p->groups.push_back({n, start[size_t(n)], c, entry, persistent});
+    }
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->plain_ids, ids.data(), size_t(arrays) * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_error(e, "upload plain ids");
+    return B200S_OK;
+}
+
+b200s_status b200s_sort_ragged_plain(b200s_plan* p, const void* d_in, void* d_out, const int32_t* d_offsets,
+                                     void* stream) {
+    if (!p || !d_in || !d_out || !d_offsets) return set_error(B200S_ERR_INVALID_ARGUMENT, "null argument");
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (const auto& g : p->groups) {
+        const KernelEntry& k = registry()[size_t(g.entry)];
+        e = k.launch_list(d_in, d_out, d_offsets, p->plain_ids + g.first, g.count, st);
+        if (e != cudaSuccess) return cuda_error(e, "per-length launch");
+    }
+    return B200S_OK;
+}
+
+int32_t b200s_plan_plain_launches(const b200s_plan* p) { return p ? int32_t(p->groups.size()) : 0; }
+
+}  // extern "C"

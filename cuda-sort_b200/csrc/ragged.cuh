@@ -1,0 +1,255 @@
+// Ragged (CSR) batches in one persistent, length-bucketed launch.
+//
+// Array a occupies elements [off[a], off[a+1]) of the flat buffer.  The
+// launch sequence of a plan is
+//   1. reset the control block (counters, queue head),
+//   2. k_bin_count   - histogram of arrays per working-length bucket,
+//   3. k_bin_scatter - array ids grouped by bucket, largest bucket first,
+//   4. k_sort_ragged - persistent CTAs pull tasks from a device queue (one
+//                      atomicAdd per task; no waiting on other CTAs).  A task
+//                      is one CTA's worth of arrays of one bucket: the CTA
+//                      splits into teams of TPA threads, one array per team,
+//                      each team running the bitonic network of its bucket's
+//                      tile (multi-warp teams synchronise on a named barrier).
+// Tasks are ordered largest working length first, so the longest tasks start
+// early and the short ones fill the tail.  The bitonic network's cost depends
+// only on the working length, so all teams of a task finish together.
+//
+// The reference's only ragged one-launch precedent is
+// SortPartitionsAdaptive_outofplace (cusort.hpp:2309-2352), a grid-stride loop
+// over CSR partitions with one block shape and shared memory sized for the
+// largest partition; here every bucket has its own tile shape.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "network.cuh"
+
+namespace b200s {
+
+constexpr int kMaxBuckets = 16;
+constexpr int kRaggedLmin = 3;  // smallest bucket: W = 8
+
+struct RaggedCtl {
+    int count[kMaxBuckets];   // arrays per bucket
+    int cursor[kMaxBuckets];  // scatter cursors
+    int head;                 // task queue head
+    int too_long;             // arrays longer than the largest bucket (not sorted)
+    int reserved[6];
+};
+
+__device__ __forceinline__ int ceil_log2_dev(int n) { return n <= 1 ? 0 : 32 - __clz(n - 1); }
+
+// Bucket of an array of length n >= 1: log2 of its working length, minus lmin.
+__device__ __forceinline__ int bucket_of(int n, int lmin) {
+    const int l = ceil_log2_dev(n);
+    return (l > lmin ? l : lmin) - lmin;
+}
+
+// The binning kernels are defined in exactly one translation unit (plan.cu).
+#ifdef B200S_DEFINE_BIN_KERNELS
+__global__ void k_bin_count(const int* __restrict__ off, int arrays, RaggedCtl* ctl, int nb) {
+    __shared__ int h[kMaxBuckets];
+    __shared__ int over;
+    if (threadIdx.x < kMaxBuckets) h[threadIdx.x] = 0;
+    if (threadIdx.x == 0) over = 0;
+    __syncthreads();
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < arrays; a += gridDim.x * blockDim.x) {
+        const int n = off[a + 1] - off[a];
+        if (n <= 0) continue;
+        const int b = bucket_of(n, kRaggedLmin);
+        if (b >= nb) atomicAdd(&over, 1);
+        else atomicAdd(&h[b], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < nb && h[threadIdx.x]) atomicAdd(&ctl->count[threadIdx.x], h[threadIdx.x]);
+    if (threadIdx.x == 0 && over) atomicAdd(&ctl->too_long, over);
+}
+
+// ids[] receives array ids grouped by bucket, largest working length first.
+__global__ void k_bin_scatter(const int* __restrict__ off, int arrays, RaggedCtl* ctl, int* ids, int nb) {
+    __shared__ int base[kMaxBuckets], h[kMaxBuckets], grab[kMaxBuckets];
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int b = nb - 1; b >= 0; --b) {
+            base[b] = s;
+            s += ctl->count[b];
+        }
+    }
+    for (int a0 = blockIdx.x * blockDim.x; a0 < arrays; a0 += gridDim.x * blockDim.x) {
+        if (threadIdx.x < kMaxBuckets) h[threadIdx.x] = 0;
+        __syncthreads();
+        const int a = a0 + int(threadIdx.x);
+        int b = -1, local = 0;
+        if (a < arrays) {
+            const int n = off[a + 1] - off[a];
+            if (n > 0) {
+                b = bucket_of(n, kRaggedLmin);
+                if (b < nb) local = atomicAdd(&h[b], 1);
+                else b = -1;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < nb && h[threadIdx.x]) grab[threadIdx.x] = atomicAdd(&ctl->cursor[threadIdx.x], h[threadIdx.x]);
+        __syncthreads();
+        if (b >= 0) ids[base[b] + grab[b] + local] = a;
+        __syncthreads();
+    }
+}
+#endif  // B200S_DEFINE_BIN_KERNELS
+
+constexpr int log2_const(int x) { return x <= 1 ? 0 : 1 + log2_const(x / 2); }
+
+// log2 elements per thread of bucket L (= log2 W) in a shape family with
+// K = 2^LKF: K elements per thread when a whole team fits the CTA, more when
+// it would not (the team never exceeds the CTA).
+constexpr int family_lk(int L, int LKF, int LOGCTA) {
+    const int lk = L < LKF ? L : LKF;
+    return L - lk > LOGCTA ? L - LOGCTA : lk;
+}
+
+// Tile of bucket L in a shape family: one lane for W <= K, then more lanes,
+// then more warps.
+template <int LKF, int L, int CTA>
+struct FamilyShape {
+    static constexpr int LK = family_lk(L, LKF, log2_const(CTA));
+    static constexpr int REST = L - LK;
+    static constexpr int LG = REST < 5 ? REST : 5;
+    static constexpr int LW = REST - LG;
+    using type = Shape<LK, LG, LW>;
+};
+
+template <class E, class S, int CTA>
+__device__ __forceinline__ void ragged_task(const typename E::Mem* in, typename E::Mem* out,
+                                            const int* __restrict__ off, const int* __restrict__ ids,
+                                            int first_id, int count, int local_task,
+                                            unsigned char* smem_raw) {
+    using R = typename E::Reg;
+    static_assert(CTA % S::TPA == 0, "whole teams per CTA");
+    constexpr int APT = CTA / S::TPA;
+    const int team = int(threadIdx.x) / S::TPA;
+    const int t = int(threadIdx.x) % S::TPA;
+    const int idx = local_task * APT + team;
+    int na = 0;
+    long long start = 0;
+    if (idx < count) {
+        const int a = ids[first_id + idx];
+        start = off[a];
+        na = off[a + 1] - off[a];
+    }
+    R* cur = reinterpret_cast<R*>(smem_raw) + size_t(team) * 2 * S::W;
+    R* nxt = cur + S::W;
+    R v[S::K];
+    load_tile<E, S::K>(v, in + start, t * S::K, na);
+    if constexpr (S::LW > 0) {
+        static_assert(CTA / S::TPA <= 15, "named barrier ids");
+        network<E, S>(v, t, cur, nxt, TeamBarrier{1 + team, S::TPA});
+    } else {
+        network<E, S>(v, t, cur, nxt);
+    }
+    store_tile<E, S::K>(v, out + start, t * S::K, na);
+}
+
+// NB buckets (W = 8 .. 8 << (NB-1)); bucket b uses family B (K = 2^LKB)
+// when bit b of family_mask is set, else family A (K = 2^LKA).
+template <class E, int CTA, int NB, int LKA, int LKB>
+__global__ void __launch_bounds__(CTA, 1) k_sort_ragged(const typename E::Mem* in, typename E::Mem* out,
+                                                        const int* __restrict__ off,
+                                                        const int* __restrict__ ids, RaggedCtl* ctl,
+                                                        unsigned family_mask) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_first[NB], s_tasks[NB], s_base[NB], s_count[NB];
+    __shared__ int s_total, s_task;
+    if (threadIdx.x == 0) {
+        int task = 0, base = 0;
+        for (int b = NB - 1; b >= 0; --b) {
+            const int c = ctl->count[b];
+            const int L = b + kRaggedLmin;
+            const int lk = family_lk(L, ((family_mask >> b) & 1u) ? LKB : LKA, log2_const(CTA));
+            const int tpa = 1 << (L - lk);
+            const int apt = CTA / tpa;
+            s_first[b] = task;
+            s_tasks[b] = (c + apt - 1) / apt;
+            s_base[b] = base;
+            s_count[b] = c;
+            task += s_tasks[b];
+            base += c;
+        }
+        s_total = task;
+    }
+    __syncthreads();
+    const int total = s_total;
+    for (;;) {
+        if (threadIdx.x == 0) s_task = atomicAdd(&ctl->head, 1);
+        __syncthreads();
+        const int task = s_task;
+        __syncthreads();
+        if (task >= total) break;
+        int b = NB - 1;
+        while (b > 0 && task >= s_first[b] + s_tasks[b]) --b;
+        const int local = task - s_first[b];
+        const bool fam_b = (family_mask >> b) & 1u;
+        sfor<0, NB>([&](auto bc) {
+            constexpr int B = decltype(bc)::value;
+            constexpr int L = B + kRaggedLmin;
+            if (b == B) {
+                if (fam_b)
+                    ragged_task<E, typename FamilyShape<LKB, L, CTA>::type, CTA>(in, out, off, ids, s_base[B],
+                                                                                  s_count[B], local, smem_raw);
+                else
+                    ragged_task<E, typename FamilyShape<LKA, L, CTA>::type, CTA>(in, out, off, ids, s_base[B],
+                                                                                  s_count[B], local, smem_raw);
+            }
+        });
+    }
+}
+
+// Shared memory of k_sort_ragged: the largest per-CTA double buffer over the
+// buckets that use it.
+template <class E, int CTA, int NB, int LKA, int LKB>
+constexpr size_t ragged_smem() {
+    size_t best = 0;
+    for (int b = 0; b < NB; ++b) {
+        const int L = b + kRaggedLmin;
+        for (int lkf : {LKA, LKB}) {
+            const int k = family_lk(L, lkf, log2_const(CTA));
+            const int rest = L - k;
+            const int lw = rest > 5 ? rest - 5 : 0;
+            if (lw > 0) {
+                const size_t bytes = 2 * size_t(CTA) * (size_t(1) << k) * sizeof(typename E::Reg);
+                if (bytes > best) best = bytes;
+            }
+        }
+    }
+    return best;
+}
+
+// Plain per-length launches: every array of the id list has the same length
+// class; one group per array, grid covers the list.
+template <class E, class S, int CTA>
+__global__ void __launch_bounds__(CTA) k_sort_idlist(const typename E::Mem* in, typename E::Mem* out,
+                                                     const int* __restrict__ off, const int* __restrict__ ids,
+                                                     int count) {
+    using R = typename E::Reg;
+    constexpr int APC = CTA / S::TPA;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* cur = reinterpret_cast<R*>(smem_raw);
+    R* nxt = cur + S::W;
+    const int slot = int(threadIdx.x) / S::TPA;
+    const int t = int(threadIdx.x) % S::TPA;
+    for (long long first = (long long)blockIdx.x * APC; first < count; first += (long long)gridDim.x * APC) {
+        const long long g = first + slot;
+        int na = 0;
+        long long start = 0;
+        if (g < count) {
+            const int a = ids[g];
+            start = off[a];
+            na = off[a + 1] - off[a];
+        }
+        R v[S::K];
+        load_tile<E, S::K>(v, in + start, t * S::K, na);
+        network<E, S>(v, t, cur, nxt);
+        store_tile<E, S::K>(v, out + start, t * S::K, na);
+    }
+}
+
+}  // namespace b200s

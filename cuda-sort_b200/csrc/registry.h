@@ -13,10 +13,9 @@ namespace b200s {
 using PackedLaunch = cudaError_t (*)(const void* in, void* out, int n, long long arrays,
                                      long long grid, cudaStream_t stream);
 using AttrQuery = cudaError_t (*)(cudaFuncAttributes* attr);
-// Launch over an explicit list of array starts (ragged batches).
-using ListLaunch = cudaError_t (*)(const void* in, void* out, const long long* d_start,
-                                   const int* d_len, const int* d_ids, long long count,
-                                   long long grid, cudaStream_t stream);
+// Launch over a list of array ids of a CSR batch (plain per-length launches).
+using ListLaunch = cudaError_t (*)(const void* in, void* out, const int* d_off, const int* d_ids,
+                                   int count, cudaStream_t stream);
 
 struct KernelEntry {
     int dtype;        // b200s_dtype
@@ -37,5 +36,27 @@ void register_rec(std::vector<KernelEntry>& out);
 void register_u64(std::vector<KernelEntry>& out);
 
 const std::vector<KernelEntry>& registry();
+
+struct RaggedCtl;
+
+// The persistent ragged kernel of one element type.
+using RaggedLaunch = cudaError_t (*)(const void* in, void* out, const int* d_off, const int* d_ids,
+                                     RaggedCtl* ctl, unsigned family_mask, int grid, cudaStream_t stream);
+struct RaggedEntry {
+    int dtype;
+    int stable;
+    int cta;          // threads per CTA
+    int nb;           // buckets: W = 8 .. 8 << (nb - 1)
+    int lka, lkb;     // log2 elements per thread of shape families A and B
+    size_t smem;      // dynamic shared memory bytes
+    RaggedLaunch launch;
+    int (*resident_per_sm)();  // CTAs per SM (occupancy), 0 on error
+};
+
+void register_ragged_i32(std::vector<RaggedEntry>& out);
+void register_ragged_rec(std::vector<RaggedEntry>& out);
+void register_ragged_u64(std::vector<RaggedEntry>& out);
+
+const std::vector<RaggedEntry>& ragged_registry();
 
 }  // namespace b200s

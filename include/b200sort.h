@@ -67,6 +67,8 @@ typedef enum b200s_dtype {
 #define B200S_STABLE 1u       /* ties keep input order (bit-exact std::stable_sort) */
 #define B200S_SORTED_CHECK 2u /* accepted for source compatibility with the reference's
                                  `Sorted` switch; the output is identical either way   */
+#define B200S_PLAN_NO_GRAPH 0x100u /* plan flag: launch the ragged sequence directly
+                                      instead of replaying a captured CUDA graph */
 
 /* A tile shape: how one array is laid over threads.  K = 2^log2_items
  * elements per thread, 2^log2_lanes lanes per array inside a warp, and
@@ -94,9 +96,11 @@ int32_t b200s_tile_count(b200s_dtype dtype, uint32_t flags);
 b200s_status b200s_tile_get(b200s_dtype dtype, uint32_t flags, int32_t index, b200s_tile* out);
 /* Tile the library uses for arrays of length n when the caller passes none. */
 b200s_status b200s_default_tile(b200s_dtype dtype, uint32_t flags, int32_t n, b200s_tile* out);
-/* Replace rows of the default tile table from a CSV file (dtype,flags,log2_w,
- * log2_items,log2_lanes,log2_warps,persistent per line; '#' comments).  Returns
- * the number of rows applied in *applied. */
+/* Replace rows of the default tile table from a CSV file; '#' starts a
+ * comment.  Packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps
+ * [,persistent].  Ragged rows: r,dtype,flags,log2_w,family (0: the larger
+ * per-thread tile, 1: the smaller one), read by plans created afterwards.
+ * Returns the number of rows applied in *applied. */
 b200s_status b200s_load_tile_table(const char* path, int32_t* applied);
 
 /* Sort `arrays` independent arrays of n elements each, packed back to back
@@ -105,6 +109,34 @@ b200s_status b200s_load_tile_table(const char* path, int32_t* applied);
 b200s_status b200s_sort_packed(b200s_dtype dtype, const void* d_in, void* d_out, int32_t n,
                                int64_t arrays, uint32_t flags, const b200s_tile* tile,
                                void* stream);
+
+/* ---- ragged batches (CSR offsets) ----------------------------------------
+ * Array a occupies elements [offsets[a], offsets[a+1]) of the flat buffer
+ * (int32 offsets, arrays + 1 entries, non-decreasing).  A plan owns the
+ * scratch of the bucketed launch (a control block and 2 * max_arrays ids)
+ * and, unless B200S_PLAN_NO_GRAPH is set, a CUDA graph of the launch
+ * sequence, re-captured when the buffers or the array count change.  Replaces
+ * the reference's partition sort over CSR partitions
+ * (SortPartitionsAdaptive_outofplace, cusort.hpp:2309-2352). */
+typedef struct b200s_plan b200s_plan;
+b200s_status b200s_plan_create(b200s_plan** out, b200s_dtype dtype, uint32_t flags, int64_t max_arrays,
+                               int32_t device);
+b200s_status b200s_plan_destroy(b200s_plan* plan);
+/* Longest array the ragged path sorts; longer arrays are counted, not sorted. */
+int32_t b200s_ragged_max_length(b200s_dtype dtype, uint32_t flags);
+/* One persistent, length-bucketed launch (graph-replayed). */
+b200s_status b200s_sort_ragged(b200s_plan* plan, const void* d_in, void* d_out, const int32_t* d_offsets,
+                               int64_t arrays, void* stream);
+/* Arrays of the last b200s_sort_ragged that exceeded b200s_ragged_max_length
+ * (synchronises `stream`). */
+b200s_status b200s_plan_too_long(b200s_plan* plan, void* stream, int64_t* count);
+/* Plain per-length form, for comparison: prepare groups the arrays by exact
+ * length on the host (from host offsets) and uploads the id lists; each sort
+ * then issues one launch per distinct length. */
+b200s_status b200s_plan_prepare_plain(b200s_plan* plan, const int32_t* h_offsets, int64_t arrays);
+b200s_status b200s_sort_ragged_plain(b200s_plan* plan, const void* d_in, void* d_out,
+                                     const int32_t* d_offsets, void* stream);
+int32_t b200s_plan_plain_launches(const b200s_plan* plan);
 
 /* ---- host-buffer entry point (end to end) ------------------------------- */
 typedef struct b200s_session b200s_session;

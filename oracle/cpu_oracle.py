@@ -105,6 +105,9 @@ def ref_cpu():
         h.ref_cpu_sort.restype = ctypes.c_int
         h.ref_cpu_sort.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong,
                                    ctypes.c_int]
+        h.ref_cpu_sort_ragged.restype = ctypes.c_int
+        h.ref_cpu_sort_ragged.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong,
+                                          ctypes.c_int]
         _ref_cpu = h
     return _ref_cpu
 
@@ -113,6 +116,13 @@ def ref_cpu_sort_inplace(type_code, data, n, arrays, threads):
     """The reference's per-array std::sort (bench.cu:300-301), in place."""
     if ref_cpu().ref_cpu_sort(type_code, _ptr(data), n, arrays, threads) != 0:
         raise ValueError("ref_cpu_sort rejected its arguments")
+
+
+def ref_cpu_sort_ragged_inplace(type_code, data, offsets, threads):
+    """The reference's std::sort applied to every array of a CSR batch, in place."""
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    if ref_cpu().ref_cpu_sort_ragged(type_code, _ptr(data), _ptr(off), len(off) - 1, threads) != 0:
+        raise ValueError("ref_cpu_sort_ragged rejected its arguments")
 
 
 def ref_gpu_available():

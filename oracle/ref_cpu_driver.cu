@@ -33,9 +33,35 @@ void sort_arrays(T* data, long long n, long long arrays, int threads) {
     }
     for (auto& th : pool) th.join();
 }
+
+template <class T>
+void sort_ragged(T* data, const long long* off, long long arrays, int threads) {
+    auto work = [&](long long lo, long long hi) {
+        for (long long a = lo; a < hi; ++a) std::sort(data + off[a], data + off[a + 1]);
+    };
+    if (threads <= 1) {
+        work(0, arrays);
+        return;
+    }
+    // Interleaved chunks of 64 arrays balance long and short arrays.
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&, t] {
+            for (long long lo = 64LL * t; lo < arrays; lo += 64LL * threads) work(lo, std::min(arrays, lo + 64));
+        });
+    for (auto& th : pool) th.join();
+}
 }  // namespace
 
 extern "C" {
+// Ragged batch (CSR offsets, arrays + 1 entries), in place.
+int ref_cpu_sort_ragged(int type, void* data, const long long* off, long long arrays, int threads) {
+    if (type == 0) sort_ragged(static_cast<int*>(data), off, arrays, threads);
+    else if (type == 1) sort_ragged(static_cast<IntAndData*>(data), off, arrays, threads);
+    else return 1;
+    return 0;
+}
+
 // type 0: int keys, type 1: IntAndData records.  Sorts in place.
 int ref_cpu_sort(int type, void* data, long long n, long long arrays, int threads) {
     if (type == 0) sort_arrays(static_cast<int*>(data), n, arrays, threads);
