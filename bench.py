@@ -16,7 +16,8 @@ Workloads: int32_4096x1024 (default), records_n{32,129,256,1000,2048,4096}
 (IntAndData records, 4194304 per batch), ragged_200000 (200000 CSR arrays,
 lengths log-uniform in [1, 8192], records; the persistent bucketed launch
 replayed from its CUDA graph, with the plain per-length launches timed
-beside it).
+beside it), cluster_256x65536 / cluster_u64_256x65536 (256 arrays of 65536
+records with int32 / uint64 keys, one 8-CTA thread-block cluster per array).
 
 --impl reference times the reference's own CPU path on this host (one
 std::sort per array over all host threads, compiled from the reference's
@@ -53,6 +54,11 @@ WORKLOADS = {
 for _n in (32, 129, 256, 1000, 2048, 4096):
     WORKLOADS["records_n%d" % _n] = dict(kind="packed", dtype=bs.I32_I32, n=_n, arrays=4194304 // _n,
                                          dist="uniform", flags=0)
+# arrays larger than one CTA: thread-block clusters
+WORKLOADS["cluster_256x65536"] = dict(kind="packed", dtype=bs.I32_I32, n=65536, arrays=256, dist="uniform",
+                                      flags=0)
+WORKLOADS["cluster_u64_256x65536"] = dict(kind="packed", dtype=bs.U64_I32, n=65536, arrays=256,
+                                          dist="uniform", flags=0)
 DTYPE_NAMES = {bs.I32: "int32", bs.I32_I32: "int32+int32", bs.U64: "uint64", bs.U64_I32: "uint64+int32"}
 
 

@@ -39,18 +39,19 @@ STATUS_NAMES = {0: "OK", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED", 3: "CUDA", 4: 
 class Tile(ctypes.Structure):
     _fields_ = [("log2_items", ctypes.c_int32), ("log2_lanes", ctypes.c_int32),
                 ("log2_warps", ctypes.c_int32), ("cta_threads", ctypes.c_int32),
-                ("persistent", ctypes.c_int32)]
+                ("persistent", ctypes.c_int32), ("log2_ctas", ctypes.c_int32)]
 
     def as_tuple(self):
-        return (self.log2_items, self.log2_lanes, self.log2_warps)
+        return (self.log2_items, self.log2_lanes, self.log2_warps, self.log2_ctas)
 
     def __repr__(self):
-        return "Tile(K=%d, lanes=%d, warps=%d, cta=%d%s)" % (
-            1 << self.log2_items, 1 << self.log2_lanes, 1 << self.log2_warps, self.cta_threads,
-            ", persistent" if self.persistent else "")
+        return "Tile(K=%d, lanes=%d, warps=%d, ctas=%d, cta=%d%s)" % (
+            1 << self.log2_items, 1 << self.log2_lanes, 1 << self.log2_warps, 1 << self.log2_ctas,
+            self.cta_threads, ", persistent" if self.persistent else "")
 
     def with_persistent(self, on=True):
-        return Tile(self.log2_items, self.log2_lanes, self.log2_warps, self.cta_threads, 1 if on else 0)
+        return Tile(self.log2_items, self.log2_lanes, self.log2_warps, self.cta_threads, 1 if on else 0,
+                    self.log2_ctas)
 
 
 class B200SortError(RuntimeError):

@@ -60,6 +60,9 @@ const std::vector<KernelEntry>& registry() {
         register_i32(v);
         register_rec(v);
         register_u64(v);
+        register_cluster_keys(v);
+        register_cluster_rec(v);
+        register_cluster_u64rec(v);
         return v;
     }();
     return all;
@@ -125,7 +128,7 @@ int lookup_tile(int dtype, int stable, const b200s_tile& tile) {
     for (size_t i = 0; i < reg.size(); ++i) {
         const KernelEntry& e = reg[i];
         if (e.dtype == dtype && e.stable == stable && e.lk == tile.log2_items &&
-            e.lg == tile.log2_lanes && e.lw == tile.log2_warps)
+            e.lg == tile.log2_lanes && e.lw == tile.log2_warps && std::max(e.lc, 0) == tile.log2_ctas)
             return int(i);
     }
     return -1;
@@ -137,6 +140,7 @@ void fill_tile(const KernelEntry& e, int persistent, b200s_tile* out) {
     out->log2_warps = e.lw;
     out->cta_threads = e.cta;
     out->persistent = persistent;
+    out->log2_ctas = std::max(e.lc, 0);
 }
 
 bool valid_dtype(int d) { return d >= 0 && d <= 3; }
@@ -291,7 +295,7 @@ b200s_status b200s_load_tile_table(const char* path, int32_t* applied) {
             return set_error(B200S_ERR_INVALID_ARGUMENT,
                              "tile table line " + std::to_string(lineno) + ": bad dtype or log2_w");
         const int stable = effective_stable(d, uint32_t(fl));
-        const b200s_tile tile{lk, lg, lw, 0, 0};
+        const b200s_tile tile{lk, lg, lw, 0, 0, 0};
         const int idx = lookup_tile(d, stable, tile);
         if (idx < 0 || registry()[size_t(idx)].log2w < w)
             return set_error(B200S_ERR_UNSUPPORTED,

@@ -4,6 +4,7 @@
 
 #include <atomic>
 
+#include "cluster.cuh"
 #include "network.cuh"
 #include "ragged.cuh"
 #include "registry.h"
@@ -83,7 +84,83 @@ struct Packed {
     static KernelEntry entry(int dtype) {
         return KernelEntry{dtype,   E::kStable ? 1 : 0, LK,     LG,         LW,
                            CTA,     S::LOGW,            SMEM,   CTA / S::TPA, &launch,
-                           &attrs,  &launch_list,       &launch_pf};
+                           &attrs,  &launch_list,       &launch_pf, -1,   nullptr};
+    }
+};
+
+// A cluster of 2^LC CTAs per array (SB: single-buffered shared memory).
+template <class E, int LK, int LG, int LW, int LC, bool SB>
+struct ClusterTile {
+    using S = Shape<LK, LG, LW>;
+    static constexpr int CTA = S::TPA;
+    static constexpr int C = 1 << LC;
+    static constexpr size_t SMEM = (SB ? 1 : 2) * size_t(S::W) * sizeof(typename E::Reg);
+
+    static cudaLaunchConfig_t config(long long clusters, cudaStream_t st, cudaLaunchAttribute* attr) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(clusters * C), 1, 1);
+        cfg.blockDim = dim3(CTA, 1, 1);
+        cfg.dynamicSmemBytes = SMEM;
+        cfg.stream = st;
+        attr->id = cudaLaunchAttributeClusterDimension;
+        attr->val.clusterDim.x = C;
+        attr->val.clusterDim.y = 1;
+        attr->val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cfg;
+    }
+    // Clusters resident at once on this device (cached per device).
+    static cudaError_t resident(int* out) {
+        static std::atomic<int> cache[64];
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        int v = cache[dev & 63].load(std::memory_order_relaxed);
+        if (v == 0) {
+            auto fn = k_sort_cluster<E, S, LC, SB>;
+            e = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(SMEM));
+            if (e != cudaSuccess) return e;
+            cudaLaunchAttribute attr;
+            cudaLaunchConfig_t cfg = config(1, nullptr, &attr);
+            e = cudaOccupancyMaxActiveClusters(&v, fn, &cfg);
+            if (e != cudaSuccess) return e;
+            if (v <= 0) return cudaErrorInvalidConfiguration;
+            cache[dev & 63].store(v, std::memory_order_relaxed);
+        }
+        *out = v;
+        return cudaSuccess;
+    }
+    static cudaError_t run(const void* in, void* out, int n, long long arrays, const int* off, const int* ids,
+                           const int* d_count, long long clusters, cudaStream_t st) {
+        int cap = 0;
+        cudaError_t e = resident(&cap);
+        if (e != cudaSuccess) return e;
+        clusters = clusters < cap ? clusters : cap;
+        if (clusters < 1) clusters = 1;
+        cudaLaunchAttribute attr;
+        cudaLaunchConfig_t cfg = config(clusters, st, &attr);
+        return cudaLaunchKernelEx(&cfg, k_sort_cluster<E, S, LC, SB>, static_cast<const typename E::Mem*>(in),
+                                  static_cast<typename E::Mem*>(out), n, arrays, off, ids, d_count);
+    }
+    static cudaError_t launch(const void* in, void* out, int n, long long arrays, long long, cudaStream_t st) {
+        return run(in, out, n, arrays, nullptr, nullptr, nullptr, arrays, st);
+    }
+    static cudaError_t launch_list(const void* in, void* out, const int* off, const int* ids, int count,
+                                   cudaStream_t st) {
+        return run(in, out, 0, count, off, ids, nullptr, count, st);
+    }
+    static cudaError_t launch_cluster_list(const void* in, void* out, const int* off, const int* ids,
+                                           const int* d_count, int max_count, cudaStream_t st) {
+        return run(in, out, 0, max_count, off, ids, d_count, max_count, st);
+    }
+    static cudaError_t attrs(cudaFuncAttributes* a) {
+        return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(k_sort_cluster<E, S, LC, SB>));
+    }
+    static KernelEntry entry(int dtype) {
+        return KernelEntry{dtype, E::kStable ? 1 : 0, LK, LG, LW, CTA, S::LOGW + LC, SMEM, 1, &launch, &attrs,
+                           &launch_list, &launch, LC, &launch_cluster_list};
     }
 };
 

@@ -71,6 +71,15 @@ struct Shape {
     static_assert(LW == 0 || LG == 5, "an array spanning warps uses whole warps");
 };
 
+// Barrier policies may set kSingleBuffer: then a shared-memory layer publishes
+// into one buffer and synchronises again after reading it (two barriers, half
+// the shared memory); otherwise it alternates two buffers with one barrier.
+template <class Bar, class = void>
+struct single_buffer : std::false_type {};
+template <class Bar>
+struct single_buffer<Bar, std::void_t<decltype(Bar::kSingleBuffer)>>
+    : std::integral_constant<bool, Bar::kSingleBuffer> {};
+
 // One comparator layer with partner mask MASK (compile-time).
 template <class E, class S, unsigned MASK, class Bar>
 __device__ __forceinline__ void layer(typename E::Reg (&v)[S::K], const int t,
@@ -122,9 +131,13 @@ __device__ __forceinline__ void layer(typename E::Reg (&v)[S::K], const int t,
             const R b = cur[(q ^ int(RM)) * S::TPA + (t ^ int(TM))];
             v[q] = E::pick(v[q], b, upper);
         });
-        R* tmp = cur;
-        cur = nxt;
-        nxt = tmp;
+        if constexpr (single_buffer<Bar>::value) {
+            bar();
+        } else {
+            R* tmp = cur;
+            cur = nxt;
+            nxt = tmp;
+        }
     }
 }
 

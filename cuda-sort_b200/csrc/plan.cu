@@ -76,7 +76,12 @@ struct b200s_plan {
     void* scratch = nullptr;
     RaggedCtl* ctl = nullptr;
     int* ids = nullptr;
+    int* oids = nullptr;          // cluster-bucket id lists, stride max_arrays
+    BinSpec spec = {};
+    int over_entry[kMaxOverflow] = {};  // registry index of each cluster bucket
     cudaStream_t capture = nullptr;
+    cudaStream_t side = nullptr;  // cluster buckets run beside the persistent kernel
+    cudaEvent_t fork = nullptr, join = nullptr;
     // the graph of the last (in, out, offsets, arrays)
     cudaGraphExec_t exec = nullptr;
     const void* g_in = nullptr;
@@ -99,13 +104,52 @@ b200s_status record_sequence(b200s_plan* p, const void* in, void* out, const int
     if (e != cudaSuccess) return cuda_error(e, "ragged control reset");
     const int bin_threads = 256;
     const int bin_grid = std::max(1, std::min(p->bin_grid, (arrays + bin_threads - 1) / bin_threads));
-    k_bin_count<<<bin_grid, bin_threads, 0, st>>>(off, arrays, p->ctl, p->rk->nb);
+    k_bin_count<<<bin_grid, bin_threads, 0, st>>>(off, arrays, p->ctl, p->spec);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "bin count launch");
-    k_bin_scatter<<<bin_grid, bin_threads, 0, st>>>(off, arrays, p->ctl, p->ids, p->rk->nb);
+    k_bin_scatter<<<bin_grid, bin_threads, 0, st>>>(off, arrays, p->ctl, p->ids, p->oids, p->spec);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "bin scatter launch");
+    if (p->spec.n_over > 0) {
+        // Fork: the cluster buckets run on the side stream while the
+        // persistent kernel runs on st; join before returning.
+        if ((e = cudaEventRecord(p->fork, st)) != cudaSuccess) return cuda_error(e, "fork record");
+        if ((e = cudaStreamWaitEvent(p->side, p->fork, 0)) != cudaSuccess) return cuda_error(e, "fork wait");
+        for (int i = 0; i < p->spec.n_over; ++i) {
+            const KernelEntry& k = registry()[size_t(p->over_entry[i])];
+            e = k.launch_cluster_list(in, out, off, p->oids + size_t(i) * p->spec.stride, &p->ctl->ocount[i],
+                                      int(std::min<long long>(arrays, p->max_arrays)), p->side);
+            if (e != cudaSuccess) return cuda_error(e, "cluster bucket launch");
+        }
+        if ((e = cudaEventRecord(p->join, p->side)) != cudaSuccess) return cuda_error(e, "join record");
+    }
     e = p->rk->launch(in, out, off, p->ids, p->ctl, p->family_mask, p->grid, st);
     if (e != cudaSuccess) return cuda_error(e, "ragged sort launch");
+    if (p->spec.n_over > 0 && (e = cudaStreamWaitEvent(st, p->join, 0)) != cudaSuccess)
+        return cuda_error(e, "join wait");
     return B200S_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+}  // extern "C"
+
+namespace {
+
+// Cluster kernels that extend the persistent kernel's range: consecutive
+// working lengths above its largest bucket.  Returns the number found.
+int overflow_entries(int dtype, int stable, int first_log2w, int* idx) {
+    int n = 0;
+    for (int w = first_log2w; n < kMaxOverflow; ++w, ++n) {
+        int found = -1;
+        const auto& reg = registry();
+        for (size_t i = 0; i < reg.size(); ++i)
+            if (reg[i].dtype == dtype && reg[i].stable == stable && reg[i].lc >= 0 && reg[i].log2w == w)
+                found = int(i);
+        if (found < 0) break;
+        if (idx) idx[n] = found;
+    }
+    return n;
 }
 
 }  // namespace
@@ -114,9 +158,12 @@ extern "C" {
 
 int32_t b200s_ragged_max_length(b200s_dtype dtype, uint32_t flags) {
     if (dtype < 0 || dtype > 3) return 0;
+    const int stable = effective_stable(dtype, flags);
     for (const RaggedEntry& e : ragged_registry())
-        if (e.dtype == dtype && e.stable == effective_stable(dtype, flags))
-            return int32_t(1) << (kRaggedLmin + e.nb - 1);
+        if (e.dtype == dtype && e.stable == stable) {
+            const int top = kRaggedLmin + e.nb - 1;
+            return int32_t(1) << (top + overflow_entries(dtype, stable, top + 1, nullptr));
+        }
     return 0;
 }
 
@@ -149,20 +196,28 @@ b200s_status b200s_plan_create(b200s_plan** out, b200s_dtype dtype, uint32_t fla
     p->family_mask = ragged_family_mask(dtype, stable);
     p->grid = sms * per_sm;
     p->bin_grid = sms * 4;
-    const size_t ids_bytes = size_t(std::max<long long>(1, max_arrays)) * sizeof(int);
-    e = cudaMalloc(&p->scratch, sizeof(RaggedCtl) + 2 * ids_bytes);
+    const long long stride = std::max<long long>(1, max_arrays);
+    p->spec.nb = rk->nb;
+    p->spec.over_lo = kRaggedLmin + rk->nb;
+    p->spec.n_over = overflow_entries(dtype, stable, p->spec.over_lo, p->over_entry);
+    p->spec.stride = int(stride);
+    // control block, bucketed ids, plain ids, cluster-bucket ids
+    const size_t ids_bytes = size_t(stride) * sizeof(int);
+    e = cudaMalloc(&p->scratch, sizeof(RaggedCtl) + (2 + size_t(p->spec.n_over)) * ids_bytes);
     if (e != cudaSuccess) {
         delete p;
         return cuda_error(e, "plan scratch allocation");
     }
     p->ctl = static_cast<RaggedCtl*>(p->scratch);
     p->ids = reinterpret_cast<int*>(static_cast<char*>(p->scratch) + sizeof(RaggedCtl));
-    p->plain_ids = p->ids + std::max<long long>(1, max_arrays);
-    e = cudaStreamCreateWithFlags(&p->capture, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-        cudaFree(p->scratch);
-        delete p;
-        return cuda_error(e, "capture stream");
+    p->plain_ids = p->ids + stride;
+    p->oids = p->plain_ids + stride;
+    if ((e = cudaStreamCreateWithFlags(&p->capture, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming)) != cudaSuccess) {
+        b200s_plan_destroy(p);
+        return cuda_error(e, "plan streams");
     }
     *out = p;
     return B200S_OK;
@@ -175,6 +230,9 @@ b200s_status b200s_plan_destroy(b200s_plan* p) {
     cudaDeviceSynchronize();
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->capture) cudaStreamDestroy(p->capture);
+    if (p->side) cudaStreamDestroy(p->side);
+    if (p->fork) cudaEventDestroy(p->fork);
+    if (p->join) cudaEventDestroy(p->join);
     if (p->scratch) cudaFree(p->scratch);
     delete p;
     return B200S_OK;

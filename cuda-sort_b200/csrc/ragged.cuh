@@ -27,14 +27,26 @@
 namespace b200s {
 
 constexpr int kMaxBuckets = 16;
+constexpr int kMaxOverflow = 4;
 constexpr int kRaggedLmin = 3;  // smallest bucket: W = 8
 
 struct RaggedCtl {
-    int count[kMaxBuckets];   // arrays per bucket
-    int cursor[kMaxBuckets];  // scatter cursors
-    int head;                 // task queue head
-    int too_long;             // arrays longer than the largest bucket (not sorted)
-    int reserved[6];
+    int count[kMaxBuckets];    // arrays per bucket
+    int cursor[kMaxBuckets];   // scatter cursors
+    int head;                  // task queue head
+    int too_long;              // arrays longer than every kernel (not sorted)
+    int ocount[kMaxOverflow];  // arrays per cluster bucket
+    int reserved[2];
+};
+
+// Binning parameters: nb buckets for the persistent kernel (W = 8 .. 8 <<
+// (nb-1)); arrays with log2 W in [over_lo, over_lo + n_over) go to the
+// cluster bucket log2 W - over_lo (ids at oids[bucket * stride]).
+struct BinSpec {
+    int nb;
+    int over_lo;
+    int n_over;
+    int stride;
 };
 
 __device__ __forceinline__ int ceil_log2_dev(int n) { return n <= 1 ? 0 : 32 - __clz(n - 1); }
@@ -47,7 +59,7 @@ __device__ __forceinline__ int bucket_of(int n, int lmin) {
 
 // The binning kernels are defined in exactly one translation unit (plan.cu).
 #ifdef B200S_DEFINE_BIN_KERNELS
-__global__ void k_bin_count(const int* __restrict__ off, int arrays, RaggedCtl* ctl, int nb) {
+__global__ void k_bin_count(const int* __restrict__ off, int arrays, RaggedCtl* ctl, BinSpec spec) {
     __shared__ int h[kMaxBuckets];
     __shared__ int over;
     if (threadIdx.x < kMaxBuckets) h[threadIdx.x] = 0;
@@ -57,16 +69,19 @@ __global__ void k_bin_count(const int* __restrict__ off, int arrays, RaggedCtl* 
         const int n = off[a + 1] - off[a];
         if (n <= 0) continue;
         const int b = bucket_of(n, kRaggedLmin);
-        if (b >= nb) atomicAdd(&over, 1);
-        else atomicAdd(&h[b], 1);
+        if (b < spec.nb) atomicAdd(&h[b], 1);
+        else if (ceil_log2_dev(n) - spec.over_lo >= spec.n_over) atomicAdd(&over, 1);
     }
     __syncthreads();
-    if (threadIdx.x < nb && h[threadIdx.x]) atomicAdd(&ctl->count[threadIdx.x], h[threadIdx.x]);
+    if (threadIdx.x < spec.nb && h[threadIdx.x]) atomicAdd(&ctl->count[threadIdx.x], h[threadIdx.x]);
     if (threadIdx.x == 0 && over) atomicAdd(&ctl->too_long, over);
 }
 
-// ids[] receives array ids grouped by bucket, largest working length first.
-__global__ void k_bin_scatter(const int* __restrict__ off, int arrays, RaggedCtl* ctl, int* ids, int nb) {
+// ids[] receives array ids grouped by bucket, largest working length first;
+// arrays for the cluster kernels go to their own lists.
+__global__ void k_bin_scatter(const int* __restrict__ off, int arrays, RaggedCtl* ctl, int* ids, int* oids,
+                              BinSpec spec) {
+    const int nb = spec.nb;
     __shared__ int base[kMaxBuckets], h[kMaxBuckets], grab[kMaxBuckets];
     if (threadIdx.x == 0) {
         int s = 0;
@@ -84,8 +99,16 @@ __global__ void k_bin_scatter(const int* __restrict__ off, int arrays, RaggedCtl
             const int n = off[a + 1] - off[a];
             if (n > 0) {
                 b = bucket_of(n, kRaggedLmin);
-                if (b < nb) local = atomicAdd(&h[b], 1);
-                else b = -1;
+                if (b < nb) {
+                    local = atomicAdd(&h[b], 1);
+                } else {
+                    const int ob = ceil_log2_dev(n) - spec.over_lo;
+                    if (ob < spec.n_over) {
+                        const int pos = atomicAdd(&ctl->ocount[ob], 1);
+                        oids[size_t(ob) * spec.stride + pos] = a;
+                    }
+                    b = -1;
+                }
             }
         }
         __syncthreads();

@@ -29,11 +29,19 @@ struct KernelEntry {
     AttrQuery attrs;
     ListLaunch launch_list;
     PackedLaunch launch_pf;   // persistent grid, next-array prefetch
+    int lc;                   // log2 CTAs per array (cluster kernels); -1 for single-CTA tiles
+    // Cluster kernels only: sort the arrays ids[0 .. *d_count) of a CSR batch,
+    // with the count read on the device (at most max_count).
+    cudaError_t (*launch_cluster_list)(const void* in, void* out, const int* d_off, const int* d_ids,
+                                       const int* d_count, int max_count, cudaStream_t stream);
 };
 
 void register_i32(std::vector<KernelEntry>& out);
 void register_rec(std::vector<KernelEntry>& out);
 void register_u64(std::vector<KernelEntry>& out);
+void register_cluster_keys(std::vector<KernelEntry>& out);
+void register_cluster_rec(std::vector<KernelEntry>& out);
+void register_cluster_u64rec(std::vector<KernelEntry>& out);
 
 const std::vector<KernelEntry>& registry();
 

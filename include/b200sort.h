@@ -71,9 +71,10 @@ typedef enum b200s_dtype {
                                       instead of replaying a captured CUDA graph */
 
 /* A tile shape: how one array is laid over threads.  K = 2^log2_items
- * elements per thread, 2^log2_lanes lanes per array inside a warp, and
- * 2^log2_warps warps per array.  The working length is
- * W = 2^(log2_items + log2_lanes + log2_warps) and must be >= n. */
+ * elements per thread, 2^log2_lanes lanes per array inside a warp,
+ * 2^log2_warps warps per CTA-slice of the array and 2^log2_ctas CTAs (a
+ * thread-block cluster) per array.  The working length is
+ * W = 2^(log2_items + log2_lanes + log2_warps + log2_ctas) and must be >= n. */
 typedef struct b200s_tile {
     int32_t log2_items;
     int32_t log2_lanes;
@@ -81,6 +82,8 @@ typedef struct b200s_tile {
     int32_t cta_threads; /* threads per CTA (output of the query functions) */
     int32_t persistent;  /* 0: one launch slot per array group; 1: grid sized to the
                             resident capacity, each group prefetching its next array */
+    int32_t log2_ctas;   /* CTAs per array: 0 for single-CTA tiles (cluster tiles of one
+                            CTA exist only where no single-CTA tile of that shape does) */
 } b200s_tile;
 
 const char* b200s_version(void);

@@ -56,9 +56,9 @@ def test_argument_checks_need_no_gpu(args, status):
 def test_explicit_tile_must_cover_n():
     t = bs.default_tile(bs.I32, 100)
     assert (1 << sum(t.as_tuple())) >= 100
-    short = bs.Tile(3, 0, 0, 0, 0)
+    short = bs.Tile(3, 0, 0, 0, 0, 0)
     assert bs.sort_packed_status(bs.I32, 16, 16, 100, 1, 0, short) == 2
-    bogus = bs.Tile(9, 9, 9, 0, 0)
+    bogus = bs.Tile(9, 9, 9, 0, 0, 0)
     assert bs.sort_packed_status(bs.I32, 16, 16, 10, 1, 0, bogus) == 2
 
 

@@ -146,6 +146,27 @@ def test_large_arrays_and_multiwarp_tiles():
             check(dtype, 0, data, n, 3, gpu_sort(dtype, data, n, 3))
 
 
+@pytest.mark.parametrize("dtype", ALL)
+@pytest.mark.parametrize("flags", [0, bs.STABLE])
+def test_cluster_lengths(dtype, flags):
+    # arrays spanning 2..8 CTAs of a thread-block cluster
+    top = bs.max_length(dtype, flags)
+    assert top >= 65536
+    for n in (8193, 16384, 16385, 32768, 40000, 65536, top):
+        if n > top:
+            continue
+        data = workloads.make_packed(dtype, n, 3, "distinct16", seed=n, extremes=True)
+        check(dtype, flags, data, n, 3, gpu_sort(dtype, data, n, 3, flags))
+
+
+@pytest.mark.parametrize("dtype", [bs.I32_I32, bs.U64_I32])
+@pytest.mark.parametrize("dist", ["uniform", "distinct16", "swap8"])
+def test_cluster_batch_256_by_65536(dtype, dist):
+    n, arrays = 65536, 256
+    data = workloads.make_packed(dtype, n, arrays, dist, seed=65536, extremes=True)
+    check(dtype, 0, data, n, arrays, gpu_sort(dtype, data, n, arrays))
+
+
 def test_host_session_matches_device_path():
     import torch
     with bs.Session(0) as s:
