@@ -118,6 +118,10 @@ __global__ void k_bin_scatter(const int* __restrict__ off, int arrays, RaggedCtl
         __syncthreads();
     }
 }
+#else
+__global__ void k_bin_count(const int* __restrict__ off, int arrays, RaggedCtl* ctl, BinSpec spec);
+__global__ void k_bin_scatter(const int* __restrict__ off, int arrays, RaggedCtl* ctl, int* ids, int* oids,
+                              BinSpec spec);
 #endif  // B200S_DEFINE_BIN_KERNELS
 
 constexpr int log2_const(int x) { return x <= 1 ? 0 : 1 + log2_const(x / 2); }

@@ -141,6 +141,27 @@ b200s_status b200s_sort_ragged_plain(b200s_plan* plan, const void* d_in, void* d
                                      const int32_t* d_offsets, void* stream);
 int32_t b200s_plan_plain_launches(const b200s_plan* plan);
 
+/* No counterpart in the reference.  The ragged sort of b200s_sort_ragged for
+ * callers that cannot allocate device memory: plugins inside a framework that
+ * owns all device memory through its own pool, and latency-critical loops
+ * where cudaMalloc's implicit device-wide synchronisation would stall other
+ * work.  Instead of a plan's allocation it uses one fixed scratch array
+ * compiled into the library (about 640 KiB on every GPU that loads the
+ * library, held until the process exits), so:
+ *   - at most B200S_NOALLOC_MAX_ARRAYS arrays per call; more is rejected
+ *     with B200S_ERR_INVALID_ARGUMENT;
+ *   - arrays longer than b200s_ragged_max_length(dtype, flags) are left
+ *     unsorted (there is no plan to report them);
+ *   - every call shares that scratch: calls whose work overlaps on the GPU
+ *     (different streams, different host threads) race and corrupt each
+ *     other; order them on one stream;
+ *   - the first call on each device looks up the scratch's device address and
+ *     sets kernel attributes; make that first call before any stream capture.
+ * It calls no cudaMalloc or cudaFree. */
+#define B200S_NOALLOC_MAX_ARRAYS 32768
+b200s_status b200s_sort_ragged_noalloc(b200s_dtype dtype, uint32_t flags, const void* d_in, void* d_out,
+                                       const int32_t* d_offsets, int64_t arrays, void* stream);
+
 /* ---- host-buffer entry point (end to end) ------------------------------- */
 typedef struct b200s_session b200s_session;
 b200s_status b200s_session_create(b200s_session** out, int32_t device);
