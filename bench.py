@@ -50,6 +50,7 @@ FALLBACK_HBM_GBS = 6650.0
 WORKLOADS = {
     "int32_4096x1024": dict(kind="packed", dtype=bs.I32, n=1024, arrays=4096, dist="uniform", flags=0),
     "ragged_200000": dict(kind="ragged", dtype=bs.I32_I32, arrays=200000, max_len=8192, dist="uniform", flags=0),
+    "ragged_20000": dict(kind="ragged", dtype=bs.I32_I32, arrays=20000, max_len=8192, dist="uniform", flags=0),
 }
 for _n in (32, 129, 256, 1000, 2048, 4096):
     WORKLOADS["records_n%d" % _n] = dict(kind="packed", dtype=bs.I32_I32, n=_n, arrays=4194304 // _n,
@@ -71,6 +72,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="ragged workloads: skip the per-length comparison")
     ap.add_argument("--preroll", type=float, default=1.5,
                     help="seconds of untimed sorting before the timed region, so clocks settle")
     return ap.parse_args()
@@ -376,6 +378,7 @@ def run_gpu(args, wl):
         verified = verify_ragged(dtype, data, off, got) and plan.too_long(ctx.sh) == 0
         kernel = "k_sort_ragged"
         launches = 3 * args.steps   # bin count, bin scatter, sort (one graph per step)
+    if wl["kind"] == "ragged" and not args.no_plain:
         # the plain per-length launches on the same input
         plain_launches = plan.prepare_plain(off.astype(np.int32))
         d_out.zero_()

@@ -1,10 +1,12 @@
 // C ABI of the batched sort: argument checking, tile selection, launches,
 // and the host-buffer (end-to-end) entry point.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <algorithm>
 #include <array>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <mutex>
@@ -105,8 +107,32 @@ DefaultTable build_defaults() {
     return t;
 }
 
+struct TableRows {
+    std::vector<std::array<int, 4>> packed;  // dtype*2+stable, log2w, registry index, persistent
+    std::vector<std::array<int, 4>> ragged;  // dtype, stable, log2w, family
+};
+b200s_status parse_table_file(const char* path, TableRows* out);
+void apply_packed_rows(const TableRows& rows, DefaultTable& t);
+std::string shipped_table_path();
+
+}  // namespace
+
+void set_ragged_family(int dtype, int stable, int log2w, int family);
+
+namespace {
+
 DefaultTable& table() {
-    static DefaultTable t = build_defaults();
+    static DefaultTable t = [] {
+        DefaultTable d = build_defaults();
+        const std::string path = shipped_table_path();
+        TableRows rows;
+        if (!path.empty() && std::ifstream(path).good() && parse_table_file(path.c_str(), &rows) == B200S_OK) {
+            apply_packed_rows(rows, d);
+            for (const auto& r : rows.ragged) set_ragged_family(r[0], r[1], r[2], r[3]);
+        }
+        clear_error();
+        return d;
+    }();
     return t;
 }
 
@@ -144,6 +170,73 @@ void fill_tile(const KernelEntry& e, int persistent, b200s_tile* out) {
 }
 
 bool valid_dtype(int d) { return d >= 0 && d <= 3; }
+
+}  // namespace
+
+namespace {
+
+// Tile table CSV: '#' comments; packed rows dtype,flags,log2_w,log2_items,
+// log2_lanes,log2_warps[,persistent]; ragged rows r,dtype,flags,log2_w,family.
+b200s_status parse_table_file(const char* path, TableRows* out) {
+    std::ifstream f(path);
+    if (!f) return set_error(B200S_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path);
+    std::string line;
+    int lineno = 0;
+    while (std::getline(f, line)) {
+        ++lineno;
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line.resize(hash);
+        if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
+        std::replace(line.begin(), line.end(), ',', ' ');
+        std::istringstream ss(line);
+        const size_t first = line.find_first_not_of(" \t");
+        if (line[first] == 'r') {
+            std::string tag;
+            int d, fl, w, fam;
+            if (!(ss >> tag >> d >> fl >> w >> fam) || !valid_dtype(d) || w < 3 || w > 18 || fam < 0 || fam > 1)
+                return set_error(B200S_ERR_INVALID_ARGUMENT,
+                                 "tile table line " + std::to_string(lineno) + ": bad ragged row");
+            out->ragged.push_back({d, effective_stable(d, uint32_t(fl)), w, fam});
+            continue;
+        }
+        int d, fl, w, lk, lg, lw, pers = 0;
+        if (!(ss >> d >> fl >> w >> lk >> lg >> lw))
+            return set_error(B200S_ERR_INVALID_ARGUMENT,
+                             "tile table line " + std::to_string(lineno) + ": expected 6 or 7 integers");
+        if (!(ss >> pers)) pers = 0;
+        if (!valid_dtype(d) || w < 0 || w > kMaxLog2W)
+            return set_error(B200S_ERR_INVALID_ARGUMENT,
+                             "tile table line " + std::to_string(lineno) + ": bad dtype or log2_w");
+        const int stable = effective_stable(d, uint32_t(fl));
+        const b200s_tile tile{lk, lg, lw, 0, 0, 0};
+        const int idx = lookup_tile(d, stable, tile);
+        if (idx < 0 || registry()[size_t(idx)].log2w < w)
+            return set_error(B200S_ERR_UNSUPPORTED,
+                             "tile table line " + std::to_string(lineno) + ": tile not compiled or too short");
+        out->packed.push_back({d * 2 + stable, w, idx, pers ? 1 : 0});
+    }
+    return B200S_OK;
+}
+
+void apply_packed_rows(const TableRows& rows, DefaultTable& t) {
+    for (const auto& u : rows.packed) {
+        t.pick[u[0] / 2][u[0] % 2][u[1]] = u[2];
+        t.persistent[u[0] / 2][u[0] % 2][u[1]] = u[3];
+    }
+}
+
+// The tuned table shipped beside the library (tune/b200_table.csv next to
+// libb200sort.so), or the file named by B200SORT_TILE_TABLE.
+std::string shipped_table_path() {
+    if (const char* env = std::getenv("B200SORT_TILE_TABLE")) return env;
+    Dl_info info;
+    if (dladdr(reinterpret_cast<void*>(&b200s_version), &info) && info.dli_fname) {
+        std::string lib = info.dli_fname;
+        const size_t slash = lib.rfind('/');
+        return (slash == std::string::npos ? std::string(".") : lib.substr(0, slash)) + "/tune/b200_table.csv";
+    }
+    return std::string();
+}
 
 }  // namespace
 
@@ -261,58 +354,16 @@ b200s_status b200s_default_tile(b200s_dtype dtype, uint32_t flags, int32_t n, b2
 
 b200s_status b200s_load_tile_table(const char* path, int32_t* applied) {
     if (!path) return set_error(B200S_ERR_INVALID_ARGUMENT, "b200s_load_tile_table: null path");
-    std::ifstream f(path);
-    if (!f) return set_error(B200S_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path);
-    std::string line;
-    int rows = 0, lineno = 0;
-    std::vector<std::array<int, 4>> updates;  // dtype*2+stable, log2w, index, persistent
-    std::vector<std::array<int, 4>> ragged_rows;  // dtype, stable, log2w, family
-    while (std::getline(f, line)) {
-        ++lineno;
-        const size_t hash = line.find('#');
-        if (hash != std::string::npos) line.resize(hash);
-        if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
-        std::replace(line.begin(), line.end(), ',', ' ');
-        std::istringstream ss(line);
-        const size_t first = line.find_first_not_of(" \t");
-        if (line[first] == 'r') {
-            // ragged row: r dtype flags log2_w family
-            std::string tag;
-            int d, fl, w, fam;
-            if (!(ss >> tag >> d >> fl >> w >> fam) || !valid_dtype(d) || w < 3 || w > 18 || fam < 0 || fam > 1)
-                return set_error(B200S_ERR_INVALID_ARGUMENT,
-                                 "tile table line " + std::to_string(lineno) + ": bad ragged row");
-            ragged_rows.push_back({d, effective_stable(d, uint32_t(fl)), w, fam});
-            ++rows;
-            continue;
-        }
-        int d, fl, w, lk, lg, lw, pers = 0;
-        if (!(ss >> d >> fl >> w >> lk >> lg >> lw))
-            return set_error(B200S_ERR_INVALID_ARGUMENT,
-                             "tile table line " + std::to_string(lineno) + ": expected 6 or 7 integers");
-        if (!(ss >> pers)) pers = 0;
-        if (!valid_dtype(d) || w < 0 || w > 20)
-            return set_error(B200S_ERR_INVALID_ARGUMENT,
-                             "tile table line " + std::to_string(lineno) + ": bad dtype or log2_w");
-        const int stable = effective_stable(d, uint32_t(fl));
-        const b200s_tile tile{lk, lg, lw, 0, 0, 0};
-        const int idx = lookup_tile(d, stable, tile);
-        if (idx < 0 || registry()[size_t(idx)].log2w < w)
-            return set_error(B200S_ERR_UNSUPPORTED,
-                             "tile table line " + std::to_string(lineno) + ": tile not compiled or too short");
-        updates.push_back({d * 2 + stable, w, idx, pers ? 1 : 0});
-        ++rows;
-    }
+    TableRows rows;
+    b200s_status st = parse_table_file(path, &rows);
+    if (st != B200S_OK) return st;
+    table();  // the built-in defaults and the shipped table come first
     {
         std::lock_guard<std::mutex> lock(g_table_mutex);
-        DefaultTable& t = table();
-        for (const auto& u : updates) {
-            t.pick[u[0] / 2][u[0] % 2][u[1]] = u[2];
-            t.persistent[u[0] / 2][u[0] % 2][u[1]] = u[3];
-        }
+        apply_packed_rows(rows, table());
     }
-    for (const auto& r : ragged_rows) set_ragged_family(r[0], r[1], r[2], r[3]);
-    if (applied) *applied = rows;
+    for (const auto& r : rows.ragged) set_ragged_family(r[0], r[1], r[2], r[3]);
+    if (applied) *applied = int32_t(rows.packed.size() + rows.ragged.size());
     clear_error();
     return B200S_OK;
 }

@@ -30,6 +30,62 @@ struct __align__(16) RecU64 {
     int32_t reserved;
 };
 
+// Element J of a 16-byte word, and the inverse, for each memory layout; J is
+// a compile-time index so the moves stay in registers.
+template <int J>
+__device__ __forceinline__ void from_u4(const uint4& u, int32_t& m) {
+    m = int32_t(J == 0 ? u.x : J == 1 ? u.y : J == 2 ? u.z : u.w);
+}
+template <int J>
+__device__ __forceinline__ void to_u4(uint4& u, int32_t m) {
+    if constexpr (J == 0) u.x = uint32_t(m);
+    else if constexpr (J == 1) u.y = uint32_t(m);
+    else if constexpr (J == 2) u.z = uint32_t(m);
+    else u.w = uint32_t(m);
+}
+template <int J>
+__device__ __forceinline__ void from_u4(const uint4& u, uint64_t& m) {
+    m = J == 0 ? (uint64_t(u.y) << 32 | u.x) : (uint64_t(u.w) << 32 | u.z);
+}
+template <int J>
+__device__ __forceinline__ void to_u4(uint4& u, uint64_t m) {
+    if constexpr (J == 0) {
+        u.x = uint32_t(m);
+        u.y = uint32_t(m >> 32);
+    } else {
+        u.z = uint32_t(m);
+        u.w = uint32_t(m >> 32);
+    }
+}
+template <int J>
+__device__ __forceinline__ void from_u4(const uint4& u, RecI32& m) {
+    m.key = int32_t(J == 0 ? u.x : u.z);
+    m.data = int32_t(J == 0 ? u.y : u.w);
+}
+template <int J>
+__device__ __forceinline__ void to_u4(uint4& u, const RecI32& m) {
+    if constexpr (J == 0) {
+        u.x = uint32_t(m.key);
+        u.y = uint32_t(m.data);
+    } else {
+        u.z = uint32_t(m.key);
+        u.w = uint32_t(m.data);
+    }
+}
+template <int J>
+__device__ __forceinline__ void from_u4(const uint4& u, RecU64& m) {
+    m.key = uint64_t(u.y) << 32 | u.x;
+    m.data = int32_t(u.z);
+    m.reserved = int32_t(u.w);
+}
+template <int J>
+__device__ __forceinline__ void to_u4(uint4& u, const RecU64& m) {
+    u.x = uint32_t(m.key);
+    u.y = uint32_t(m.key >> 32);
+    u.z = uint32_t(m.data);
+    u.w = uint32_t(m.reserved);
+}
+
 __device__ __forceinline__ uint32_t shfl_x(uint32_t v, int m) {
     return __shfl_xor_sync(0xffffffffu, v, m);
 }

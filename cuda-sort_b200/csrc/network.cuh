@@ -170,13 +170,18 @@ __device__ __forceinline__ void load_tile(typename E::Reg (&v)[K], const typenam
     constexpr int BYTES = K * int(sizeof(M));
     if constexpr (BYTES % 16 == 0) {
         if (base + K <= n && (reinterpret_cast<uintptr_t>(src + base) & 15u) == 0) {
-            uint4 raw[BYTES / 16];
+            constexpr int PER = 16 / int(sizeof(M));
             const uint4* p = reinterpret_cast<const uint4*>(src + base);
-#pragma unroll
-            for (int c = 0; c < BYTES / 16; ++c) raw[c] = __ldcs(p + c);
-            const M* m = reinterpret_cast<const M*>(raw);
-#pragma unroll
-            for (int q = 0; q < K; ++q) v[q] = E::from_mem(m[q], base + q);
+            sfor<0, BYTES / 16>([&](auto cc) {
+                constexpr int c = decltype(cc)::value;
+                const uint4 u = __ldcs(p + c);
+                sfor<0, PER>([&](auto jc) {
+                    constexpr int j = decltype(jc)::value;
+                    M m;
+                    from_u4<j>(u, m);
+                    v[c * PER + j] = E::from_mem(m, base + c * PER + j);
+                });
+            });
             return;
         }
     }
@@ -194,13 +199,17 @@ __device__ __forceinline__ void store_tile(const typename E::Reg (&v)[K], typena
     constexpr int BYTES = K * int(sizeof(M));
     if constexpr (BYTES % 16 == 0) {
         if (base + K <= n && (reinterpret_cast<uintptr_t>(dst + base) & 15u) == 0) {
-            uint4 raw[BYTES / 16];
-            M* m = reinterpret_cast<M*>(raw);
-#pragma unroll
-            for (int q = 0; q < K; ++q) m[q] = E::to_mem(v[q]);
+            constexpr int PER = 16 / int(sizeof(M));
             uint4* p = reinterpret_cast<uint4*>(dst + base);
-#pragma unroll
-            for (int c = 0; c < BYTES / 16; ++c) __stcs(p + c, raw[c]);
+            sfor<0, BYTES / 16>([&](auto cc) {
+                constexpr int c = decltype(cc)::value;
+                uint4 u;
+                sfor<0, PER>([&](auto jc) {
+                    constexpr int j = decltype(jc)::value;
+                    to_u4<j>(u, E::to_mem(v[c * PER + j]));
+                });
+                __stcs(p + c, u);
+            });
             return;
         }
     }
