@@ -33,7 +33,10 @@ NP_DTYPES = {
 
 OK = 0
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED", 3: "CUDA", 4: "OUT_OF_MEMORY",
-                5: "TIMEOUT", 6: "BUDGET"}
+                5: "TIMEOUT", 6: "BUDGET", 7: "BUSY", 8: "CANCELLED"}
+ERR_TIMEOUT, ERR_BUDGET, ERR_BUSY, ERR_CANCELLED = 5, 6, 7, 8
+MEM_DEVICE, MEM_HOST = 0, 1
+REQ_FREE, REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = range(6)
 
 
 class Tile(ctypes.Structure):
@@ -52,6 +55,23 @@ class Tile(ctypes.Structure):
     def with_persistent(self, on=True):
         return Tile(self.log2_items, self.log2_lanes, self.log2_warps, self.cta_threads, 1 if on else 0,
                     self.log2_ctas)
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("dtype", ctypes.c_int), ("flags", ctypes.c_uint32),
+                ("budget_bytes", ctypes.c_int64), ("max_inflight", ctypes.c_int32), ("max_batch", ctypes.c_int32),
+                ("max_queue", ctypes.c_int64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in (
+        "submitted", "completed", "failed", "cancelled", "rejected", "batches", "keys_completed", "queued",
+        "inflight_batches", "peak_arena_bytes", "arena_bytes", "max_batch_requests")] + \
+        [(n, ctypes.c_double) for n in ("mean_batch_requests", "p50_us", "p99_us", "p999_us", "max_us", "mean_us",
+                                        "span_s")]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class B200SortError(RuntimeError):
@@ -89,6 +109,20 @@ _SIGNATURES = {
     "b200s_session_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "b200s_sort_packed_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32]),
+    "b200s_server_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ServerConfig)]),
+    "b200s_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "b200s_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                           ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]),
+    "b200s_server_submit_arrived": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                                   ctypes.c_uint32, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64)]),
+    "b200s_server_clock_ns": (ctypes.c_int64, []),
+    "b200s_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int64,
+                                         ctypes.POINTER(ctypes.c_int)]),
+    "b200s_server_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32),
+                                         ctypes.POINTER(ctypes.c_int)]),
+    "b200s_server_cancel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "b200s_server_drain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    "b200s_server_stats_get": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats), ctypes.c_int32]),
 }
 
 
@@ -226,6 +260,69 @@ class Plan:
     def close(self):
         if self._h:
             lib().b200s_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching sort server (b200s_server_*): submit requests of any
+    length as they arrive; the server batches, sorts and returns them."""
+
+    def __init__(self, dtype, budget_bytes=1 << 30, max_inflight=4, max_batch=4096, max_queue=65536, flags=0,
+                 device=0):
+        self.dtype = dtype
+        self._h = ctypes.c_void_p()
+        cfg = ServerConfig(device, dtype, flags, budget_bytes, max_inflight, max_batch, max_queue)
+        check(lib().b200s_server_create(ctypes.byref(self._h), ctypes.byref(cfg)))
+
+    def submit_status(self, src, dst, n, mem=MEM_DEVICE):
+        """Raw status and ticket of one submission (src/dst are integer pointers)."""
+        t = ctypes.c_uint64(0)
+        st = lib().b200s_server_submit(self._h, ctypes.c_void_p(src), ctypes.c_void_p(dst), n, mem,
+                                       ctypes.byref(t))
+        return st, t.value
+
+    def submit(self, src, dst, n, mem=MEM_DEVICE):
+        st, t = self.submit_status(src, dst, n, mem)
+        check(st)
+        return t
+
+    def wait(self, ticket, timeout_us=-1):
+        """Outcome of a request (a status code), after it finished."""
+        r = ctypes.c_int(0)
+        check(lib().b200s_server_wait(self._h, ticket, timeout_us, ctypes.byref(r)))
+        return r.value
+
+    def poll(self, ticket):
+        state, r = ctypes.c_int32(0), ctypes.c_int(0)
+        check(lib().b200s_server_poll(self._h, ticket, ctypes.byref(state), ctypes.byref(r)))
+        return state.value, r.value
+
+    def cancel(self, ticket):
+        return lib().b200s_server_cancel(self._h, ticket)
+
+    def drain(self, timeout_us=-1):
+        return check(lib().b200s_server_drain(self._h, timeout_us))
+
+    def stats(self, reset=False):
+        s = ServerStats()
+        check(lib().b200s_server_stats_get(self._h, ctypes.byref(s), int(reset)))
+        return s
+
+    def close(self):
+        if self._h:
+            lib().b200s_server_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __enter__(self):

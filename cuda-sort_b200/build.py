@@ -26,8 +26,19 @@ def _sources():
     return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
-def _headers_mtime():
-    newest = 0.0
+def _deps_mtime(obj, path):
+    """Newest modification time among the source and the headers it included
+    at its last compile (nvcc -MD writes them to obj.d); every header when the
+    dependency file is missing."""
+    newest = os.path.getmtime(path)
+    dep = obj[:-2] + ".d"
+    if os.path.exists(dep):
+        with open(dep) as f:
+            text = f.read().replace("\\\n", " ")
+        for tok in text.split(":", 1)[-1].split():
+            if os.path.exists(tok):
+                newest = max(newest, os.path.getmtime(tok))
+        return newest
     for d in (CSRC, os.path.join(ROOT, "include")):
         for f in os.listdir(d):
             if f.endswith((".cuh", ".h", ".hpp")):
@@ -38,9 +49,9 @@ def _headers_mtime():
 def _compile(src, extra):
     obj = os.path.join(OBJ, src[:-3] + ".o")
     path = os.path.join(CSRC, src)
-    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(path), _headers_mtime()):
+    if os.path.exists(obj) and os.path.getmtime(obj) >= _deps_mtime(obj, path):
         return obj, None
-    cmd = [NVCC] + ARCH + FLAGS + extra + ["-c", path, "-o", obj]
+    cmd = [NVCC] + ARCH + FLAGS + extra + ["-MD", "-MF", obj[:-2] + ".d", "-c", path, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         return obj, "$ " + " ".join(cmd) + "\n" + r.stdout + r.stderr

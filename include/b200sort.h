@@ -53,7 +53,9 @@ typedef enum b200s_status {
     B200S_ERR_CUDA = 3,             /* a CUDA runtime call failed; see b200s_last_error() */
     B200S_ERR_OUT_OF_MEMORY = 4,    /* a session/plan/server could not allocate */
     B200S_ERR_TIMEOUT = 5,          /* a bounded wait gave up */
-    B200S_ERR_BUDGET = 6            /* request larger than the server's device-memory budget */
+    B200S_ERR_BUDGET = 6,           /* request larger than the server's device-memory budget */
+    B200S_ERR_BUSY = 7,             /* the server's request table is full; retry later */
+    B200S_ERR_CANCELLED = 8         /* result of a request cancelled before it was admitted */
 } b200s_status;
 
 typedef enum b200s_dtype {
@@ -172,6 +174,77 @@ b200s_status b200s_session_destroy(b200s_session* session);
  * bandwidth.  Returns after the output is in h_out. */
 b200s_status b200s_sort_packed_host(b200s_session* session, b200s_dtype dtype, const void* h_in,
                                     void* h_out, int32_t n, int64_t arrays, uint32_t flags);
+
+/* ---- serving: continuous batching of arriving sort requests ---------------
+ * No counterpart in the reference (it sorts batches it builds itself).  A
+ * server owns a device arena of budget_bytes and a worker thread.  Requests
+ * (one array each, of any length up to b200s_ragged_max_length) are queued by
+ * b200s_server_submit from any host thread and return at once; the worker
+ * admits queued requests into the next batch whenever one of max_inflight
+ * device slots is free and the arena has room for them, stages them into the
+ * arena, sorts the batch with the ragged kernels, and copies each result to
+ * its destination.  Batches of different slots run on different streams and
+ * overlap on the device; requests that arrive meanwhile wait in the queue and
+ * form the next batch.  A request's result is identical to sorting it alone
+ * (b200s_sort_packed with arrays = 1).  Sources and destinations stay valid
+ * until the request finishes: B200S_MEM_DEVICE pointers are device memory (or
+ * mapped pinned host memory) read and written by kernels; B200S_MEM_HOST
+ * pointers are host memory copied with cudaMemcpyAsync (pinned is faster). */
+#define B200S_MEM_DEVICE 0u
+#define B200S_MEM_HOST 1u
+
+/* request states (b200s_server_poll) */
+#define B200S_REQ_FREE 0      /* unknown ticket, or its table entry was reused */
+#define B200S_REQ_QUEUED 1
+#define B200S_REQ_RUNNING 2
+#define B200S_REQ_DONE 3
+#define B200S_REQ_FAILED 4
+#define B200S_REQ_CANCELLED 5
+
+typedef struct b200s_server_config {
+    int32_t device;
+    b200s_dtype dtype;
+    uint32_t flags;           /* B200S_STABLE */
+    int64_t budget_bytes;     /* device arena for admitted requests (default 1 GiB when 0) */
+    int32_t max_inflight;     /* batches on the device at once (default 4) */
+    int32_t max_batch;        /* requests per batch (default 4096) */
+    int64_t max_queue;        /* request table entries (default 65536) */
+} b200s_server_config;
+
+typedef struct b200s_server_stats {
+    int64_t submitted, completed, failed, cancelled, rejected;
+    int64_t batches, keys_completed, queued, inflight_batches;
+    int64_t peak_arena_bytes, arena_bytes, max_batch_requests;
+    double mean_batch_requests;
+    double p50_us, p99_us, p999_us, max_us, mean_us; /* submit -> result written */
+    double span_s;            /* first submit -> last completion */
+} b200s_server_stats;
+
+typedef struct b200s_server b200s_server;
+b200s_status b200s_server_create(b200s_server** out, const b200s_server_config* config);
+/* Cancels queued requests, waits for admitted ones, frees the arena. */
+b200s_status b200s_server_destroy(b200s_server* server);
+/* Queue one request of n elements; *ticket identifies it.  B200S_ERR_BUDGET
+ * when it can never fit the arena, B200S_ERR_BUSY when max_queue requests are
+ * pending, B200S_ERR_UNSUPPORTED beyond the longest sortable array. */
+b200s_status b200s_server_submit(b200s_server* server, const void* src, void* dst, int32_t n, uint32_t mem,
+                                 uint64_t* ticket);
+/* Same, for a request that arrived at arrival_ns (b200s_server_clock_ns
+ * timeline) before this call: its latency counts from then. */
+b200s_status b200s_server_submit_arrived(b200s_server* server, const void* src, void* dst, int32_t n,
+                                         uint32_t mem, int64_t arrival_ns, uint64_t* ticket);
+/* The server's clock (monotonic nanoseconds). */
+int64_t b200s_server_clock_ns(void);
+/* Wait for a request (timeout_us < 0: no limit); *result is its outcome
+ * (B200S_OK, B200S_ERR_CUDA, B200S_ERR_CANCELLED). */
+b200s_status b200s_server_wait(b200s_server* server, uint64_t ticket, int64_t timeout_us, b200s_status* result);
+b200s_status b200s_server_poll(b200s_server* server, uint64_t ticket, int32_t* state, b200s_status* result);
+/* Cancel a request that has not been admitted yet. */
+b200s_status b200s_server_cancel(b200s_server* server, uint64_t ticket);
+/* Wait until no request is queued or running. */
+b200s_status b200s_server_drain(b200s_server* server, int64_t timeout_us);
+/* Counters and latency percentiles since creation or the last reset. */
+b200s_status b200s_server_stats_get(b200s_server* server, b200s_server_stats* out, int32_t reset);
 
 #ifdef __cplusplus
 }
