@@ -17,13 +17,18 @@ Workloads: int32_4096x1024 (default), records_n{32,129,256,1000,2048,4096}
 lengths log-uniform in [1, 8192], records; the persistent bucketed launch
 replayed from its CUDA graph, with the plain per-length launches timed
 beside it), cluster_256x65536 / cluster_u64_256x65536 (256 arrays of 65536
-records with int32 / uint64 keys, one 8-CTA thread-block cluster per array).
+records with int32 / uint64 keys, one 8-CTA thread-block cluster per array),
+serving (a stream of sort requests of 16 .. 65536 records into the
+continuous-batching server under a 16 GB device budget: peak sustained keys/s
+in closed loop, then Poisson arrival rates with p50/p99/p99.9 latency, each
+beside per-request plain launches; --duration seconds per point).
 
 --impl reference times the reference's own CPU path on this host (one
 std::sort per array over all host threads, compiled from the reference's
 headers into oracle/_ref/) on the same workload; only rank 0 runs it.
 """
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -60,6 +65,9 @@ WORKLOADS["cluster_256x65536"] = dict(kind="packed", dtype=bs.I32_I32, n=65536, 
                                       flags=0)
 WORKLOADS["cluster_u64_256x65536"] = dict(kind="packed", dtype=bs.U64_I32, n=65536, arrays=256,
                                           dist="uniform", flags=0)
+# request stream into the server: 2048 device-resident requests reused cyclically
+WORKLOADS["serving"] = dict(kind="serving", dtype=bs.I32_I32, arrays=2048, min_len=16, max_len=65536,
+                            dist="uniform", flags=0, budget=16 << 30)
 DTYPE_NAMES = {bs.I32: "int32", bs.I32_I32: "int32+int32", bs.U64: "uint64", bs.U64_I32: "uint64+int32"}
 
 
@@ -75,6 +83,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="ragged workloads: skip the per-length comparison")
     ap.add_argument("--preroll", type=float, default=1.5,
                     help="seconds of untimed sorting before the timed region, so clocks settle")
+    ap.add_argument("--duration", type=float, default=2.0, help="serving: seconds per rate point")
+    ap.add_argument("--rates", default="1e4,3e4,1e5,3e5,1e6", help="serving: Poisson arrival rates (req/s)")
     return ap.parse_args()
 
 
@@ -192,7 +202,10 @@ def time_cpu(data, wl, threads, off=None, budget_s=8.0, min_reps=2, max_reps=50)
 def make_input(wl, seed):
     if wl["kind"] == "packed":
         return workloads.make_packed(wl["dtype"], wl["n"], wl["arrays"], wl["dist"], seed=seed), None
-    lengths = workloads.ragged_lengths(wl["arrays"], max_len=wl["max_len"], seed=seed)
+    if "min_len" in wl:
+        lengths = workloads.log_uniform_lengths(wl["arrays"], wl["min_len"], wl["max_len"], seed=seed)
+    else:
+        lengths = workloads.ragged_lengths(wl["arrays"], max_len=wl["max_len"], seed=seed)
     return workloads.make_ragged(wl["dtype"], lengths, wl["dist"], seed=seed)
 
 
@@ -205,7 +218,7 @@ def config_of(args, wl, data):
         c["n"] = wl["n"]
         c["l2"] = "inputs rotate over sets larger than L2 (126 MB)"
     else:
-        c["lengths"] = "log-uniform in [1, %d], CSR int32 offsets" % wl["max_len"]
+        c["lengths"] = "log-uniform in [%d, %d], CSR int32 offsets" % (wl.get("min_len", 1), wl["max_len"])
         c["l2"] = "input %.2f GB, larger than L2" % (data.nbytes / 1e9)
     return c
 
@@ -470,11 +483,109 @@ def run_gpu(args, wl):
     return 0 if verified else 1
 
 
+# ---- serving: request stream into the continuous-batching server -------------------
+
+class LgResult(ctypes.Structure):
+    """lg_result of the load generator (cuda-sort_b200/harness/loadgen.cpp)."""
+    _fields_ = [(n, ctypes.c_int64) for n in ("submitted", "completed", "rejected", "batches", "peak_arena_bytes")] + \
+        [(n, ctypes.c_double) for n in ("p50_us", "p99_us", "p999_us", "max_us", "mean_us", "span_s", "keys_per_s",
+                                        "req_per_s", "offered_req_per_s", "max_lag_us", "mean_batch")] + \
+        [("overloaded", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+def run_serving(args, wl):
+    ctx = Ctx()
+    torch = ctx.torch
+    if ctx.world > 1:
+        ctx.dist.destroy_process_group()   # replicas: every rank serves its own stream
+    dtype = wl["dtype"]
+    lens = workloads.log_uniform_lengths(wl["arrays"], wl["min_len"], wl["max_len"], seed=4321 + ctx.rank)
+    data, off = workloads.make_ragged(dtype, lens, wl["dist"], seed=4321 + ctx.rank)
+    d_all = torch.from_numpy(data.view(np.uint8).copy()).to(ctx.dev)
+    o_all = torch.empty_like(d_all)
+    eb = bs.ELEM_BYTES[dtype]
+    P = len(lens)
+    src = (ctypes.c_void_p * P)(*[d_all.data_ptr() + int(off[i]) * eb for i in range(P)])
+    dst = (ctypes.c_void_p * P)(*[o_all.data_ptr() + int(off[i]) * eb for i in range(P)])
+    c_lens = (ctypes.c_int32 * P)(*[int(x) for x in lens])
+    lg = ctypes.CDLL(os.path.join(ROOT, "cuda-sort_b200", "libb200sort_loadgen.so"))
+    lg.lg_run.restype = ctypes.c_int
+    lg.lg_run.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                          ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                          ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(LgResult)]
+    SERVER_OPEN, PLAIN_OPEN, SERVER_CLOSED, PLAIN_CLOSED = 0, 1, 2, 3
+    srv = bs.Server(dtype, budget_bytes=wl["budget"], max_inflight=4, max_batch=4096, max_queue=1 << 20,
+                    device=ctx.local)
+
+    def run(mode, rate=0.0, window=0, duration=args.duration, seed=1):
+        r = LgResult()
+        rc = lg.lg_run(mode, srv._h if mode in (SERVER_OPEN, SERVER_CLOSED) else None, dtype, src, dst, c_lens, P,
+                       rate, duration, window, seed, 1.0, ctypes.byref(r))
+        if rc != 0:
+            raise RuntimeError("load generator mode %d failed with %d: %s" % (mode, rc, bs.lib().b200s_last_error()))
+        return r
+
+    clocks_sampler = ClockSampler(None)
+    try:
+        uuid = str(torch.cuda.get_device_properties(ctx.dev).uuid)
+        clocks_sampler = ClockSampler(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+    except Exception:
+        pass
+    # warm-up: every kernel and both paths once, untimed
+    run(SERVER_CLOSED, window=1024, duration=0.5)
+    run(PLAIN_CLOSED, window=256, duration=0.3)
+    clocks_sampler.start()
+    peak = run(SERVER_CLOSED, window=8192)
+    plain_peak = run(PLAIN_CLOSED, window=1024)
+    rates = [float(x) for x in args.rates.split(",") if x]
+    half = 0.5 * peak.req_per_s
+    points = []
+    for rate in rates + [half]:
+        srv_r = run(SERVER_OPEN, rate=rate, seed=int(rate) + 7)
+        pl_r = run(PLAIN_OPEN, rate=rate, seed=int(rate) + 7)
+        points.append({"offered_req_per_s": rate, "server": srv_r.as_dict(), "plain": pl_r.as_dict(),
+                       "is_half_peak": rate == half})
+    clocks_sampler.stop()
+    torch.cuda.synchronize()
+    srv.close()
+    # every pool entry holds the sort of its own input (the last request that used it)
+    got = o_all.cpu().numpy().view(bs.NP_DTYPES[dtype])
+    verified = verify_ragged(dtype, data, off, got)
+    value = peak.keys_per_s * ctx.world
+    hp = points[-1]["server"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ctx.world, "steps": len(points) + 2,
+        "warmup": 2, "ms_per_step": args.duration * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": DTYPE_NAMES[dtype], "data": "synthetic",
+        "config": {"workload": "serving", "kind": "serving", "requests_in_pool": P,
+                   "lengths": "log-uniform in [%d, %d] records" % (wl["min_len"], wl["max_len"]),
+                   "key_dtype": DTYPE_NAMES[dtype], "distribution": wl["dist"], "budget_bytes": wl["budget"],
+                   "max_inflight_batches": 4, "seconds_per_point": args.duration,
+                   "l2": "pool of %.0f MB inputs + outputs, larger than L2" % (2 * data.nbytes / 1e6)},
+        "serving": {"peak_closed_loop": peak.as_dict(), "plain_closed_loop": plain_peak.as_dict(),
+                    "peak_speedup_vs_plain": peak.keys_per_s / max(plain_peak.keys_per_s, 1.0),
+                    "half_peak_req_per_s": half, "half_peak_p99_us": hp["p99_us"],
+                    "half_peak_p99_target_met": bool(hp["p99_us"] <= 1000.0 and not hp["overloaded"]),
+                    "poisson": points},
+        "roofline": None, "cpu_baseline": None,
+        "e2e": None, "gpu_launches": int(peak.batches * 5), "clocks": clocks_sampler.summary(),
+        "verified": verified, "library": bs.version(),
+    }
+    if ctx.rank == 0:
+        print(json.dumps(line))
+    return 0 if verified else 1
+
+
 def main():
     args = parse()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         return reference_arm(args, wl)
+    if wl["kind"] == "serving":
+        return run_serving(args, wl)
     return run_gpu(args, wl)
 
 

@@ -16,6 +16,8 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libb200sort.so")
 BASELINES = os.path.join(HERE, "baselines")
 CUB_LIB = os.path.join(HERE, "libb200sort_cub.so")
+HARNESS = os.path.join(HERE, "harness")
+LOADGEN_LIB = os.path.join(HERE, "libb200sort_loadgen.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -75,8 +77,9 @@ def build(verbose=False, extra=None, jobs=None):
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
     build_cub_baseline()
+    build_loadgen()
     if verbose:
-        print("built", LIB, CUB_LIB)
+        print("built", LIB, CUB_LIB, LOADGEN_LIB)
     return LIB
 
 
@@ -90,6 +93,20 @@ def build_cub_baseline():
     if r.returncode != 0:
         raise RuntimeError("CUB baseline build failed:\n" + r.stdout + r.stderr)
     return CUB_LIB
+
+
+def build_loadgen():
+    """The serving load generator (benchmark harness over the library's C ABI)."""
+    src = os.path.join(HARNESS, "loadgen.cpp")
+    if os.path.exists(LOADGEN_LIB) and os.path.getmtime(LOADGEN_LIB) >= max(
+            os.path.getmtime(src), os.path.getmtime(LIB), os.path.getmtime(os.path.join(ROOT, "include", "b200sort.h"))):
+        return LOADGEN_LIB
+    cmd = [NVCC, "-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-I" + os.path.join(ROOT, "include"),
+           "-x", "cu", src, "-o", LOADGEN_LIB, "-L" + HERE, "-lb200sort", "-Xlinker", "-rpath,$ORIGIN"] + ARCH
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("load generator build failed:\n" + r.stdout + r.stderr)
+    return LOADGEN_LIB
 
 
 if __name__ == "__main__":

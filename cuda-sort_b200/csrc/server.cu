@@ -22,6 +22,8 @@
 //   5. k_stage (out): device-memory results copied to their destinations,
 //   6. host-memory requests: one cudaMemcpyAsync each back to the host,
 //   7. an event the scheduler polls.
+// A batch of at most kDirectMax requests instead launches the packed sort once
+// per request, straight from its source to its destination.
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -42,6 +44,7 @@ size_t elem_bytes(int dtype);
 namespace {
 
 constexpr int kChunkBytes = 16384;
+constexpr int kDirectMax = 3;  // batches of up to this many requests launch per request
 constexpr int kStageThreads = 256;
 
 struct Desc {
@@ -167,6 +170,7 @@ public:
             *err = "batch region beyond int32 offsets";
             return B200S_ERR_INVALID_ARGUMENT;
         }
+        if (count <= kDirectMax) return launch_direct(s, items, count, err);
         int32_t* off = reinterpret_cast<int32_t*>(s.h_meta);
         Desc* desc = reinterpret_cast<Desc*>(s.h_meta + offsets_bytes());
         int chunks = 0;
@@ -212,6 +216,39 @@ public:
                                     size_t(items[i].req->n) * size_t(eb_), cudaMemcpyDeviceToHost, s.stream);
                 if (e != cudaSuccess) return cuda_fail(e, "server device-to-host copy", err);
             }
+        if ((e = cudaEventRecord(s.done, s.stream)) != cudaSuccess) return cuda_fail(e, "server event record", err);
+        return B200S_OK;
+    }
+
+    // A batch of a few requests skips staging and binning: each request is
+    // one packed launch of one array, from its source into its destination
+    // (host-memory requests through their arena slot).  At low load this is
+    // the whole path; the result equals the batched path's (the network's
+    // output does not depend on the working length or the padding).
+    b200s_status launch_direct(Slot& s, const serving::Item* items, int count, std::string* err) {
+        char* arena = static_cast<char*>(arena_);
+        cudaError_t e;
+        for (int i = 0; i < count; ++i) {
+            const serving::Request& r = *items[i].req;
+            const size_t bytes = size_t(r.n) * size_t(eb_);
+            const void* in = r.src;
+            void* out = r.dst;
+            if (r.mem == B200S_MEM_HOST) {
+                out = arena + items[i].arena_elem * eb_;
+                in = out;
+                if ((e = cudaMemcpyAsync(out, r.src, bytes, cudaMemcpyHostToDevice, s.stream)) != cudaSuccess)
+                    return cuda_fail(e, "server host-to-device copy", err);
+            }
+            const b200s_status st =
+                b200s_sort_packed(b200s_dtype(dtype_), in, out, r.n, 1, flags_, nullptr, s.stream);
+            if (st != B200S_OK) {
+                *err = std::string("server request sort: ") + b200s_last_error();
+                return st;
+            }
+            if (r.mem == B200S_MEM_HOST &&
+                (e = cudaMemcpyAsync(r.dst, out, bytes, cudaMemcpyDeviceToHost, s.stream)) != cudaSuccess)
+                return cuda_fail(e, "server device-to-host copy", err);
+        }
         if ((e = cudaEventRecord(s.done, s.stream)) != cudaSuccess) return cuda_fail(e, "server event record", err);
         return B200S_OK;
     }

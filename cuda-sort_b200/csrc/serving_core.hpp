@@ -457,6 +457,7 @@ private:
 
     void loop() {
         int idle_spins = 0;
+        int64_t last_active = now_ns();
         for (;;) {
             bool progressed = retire();
             progressed = admit() || progressed;
@@ -477,9 +478,18 @@ private:
             }
             if (progressed) {
                 idle_spins = 0;
+                last_active = now_ns();
                 continue;
             }
             if (inflight_ == 0 && queue_.empty()) {
+                // Idle: keep polling for a short while (a request arriving
+                // soon after another is admitted without a thread wake-up),
+                // then sleep until a submission.
+                if (now_ns() - last_active < kIdleSpinNs) {
+                    lk.unlock();
+                    std::this_thread::yield();
+                    continue;
+                }
                 cv_work_.wait_for(lk, std::chrono::milliseconds(20));
                 continue;
             }
@@ -488,6 +498,8 @@ private:
             if (++idle_spins > 64) std::this_thread::yield();
         }
     }
+
+    static constexpr int64_t kIdleSpinNs = 200000;
 
     std::unique_ptr<B> be_;
     Limits lim_;

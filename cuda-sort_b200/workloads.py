@@ -122,11 +122,20 @@ def _assemble(dtype, flat_keys):
 
 
 def ragged_lengths(arrays, max_len=8192, seed=1234, min_len=1):
-    """Lengths log-uniform on [min_len, max_len]: floor(exp(U * ln(max_len))), clamped."""
+    """Lengths floor(exp(U * ln(max_len))), log-uniform on [1, max_len], then
+    clamped to [min_len, max_len]."""
     rng = np.random.default_rng(seed)
     u = rng.random(arrays)
     lens = np.floor(np.exp(u * np.log(max_len))).astype(np.int64)
     return np.clip(lens, min_len, max_len)
+
+
+def log_uniform_lengths(count, lo, hi, seed=1234):
+    """Lengths log-uniform on [lo, hi]: floor(exp(ln lo + U * (ln hi - ln lo)))."""
+    rng = np.random.default_rng(seed)
+    u = rng.random(count)
+    lens = np.floor(np.exp(np.log(lo) + u * (np.log(hi) - np.log(lo)))).astype(np.int64)
+    return np.clip(lens, lo, hi)
 
 
 def offsets_from_lengths(lengths):

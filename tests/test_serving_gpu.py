@@ -20,7 +20,7 @@ def make_requests(dtype, count, seed, max_len=65536):
     """Requests of lengths log-uniform in [16, max_len] (a few of each size
     class), keys from 16 distinct values plus the extremes: many ties."""
     max_len = min(max_len, bs.ragged_max_length(dtype))
-    lengths = workloads.ragged_lengths(count, max_len=max_len, seed=seed, min_len=16)
+    lengths = workloads.log_uniform_lengths(count, 16, max_len, seed=seed)
     lengths[:4] = [1, 2, 8193, max_len] if max_len >= 8193 else [1, 2, 3, max_len]
     data, off = workloads.make_ragged(dtype, lengths, "distinct16", seed=seed, extremes=True)
     return [data[off[i]:off[i + 1]].copy() for i in range(count)]
@@ -42,7 +42,7 @@ def sort_alone(srv, dtype, reqs):
         d_in = to_device(arr)
         d_out = empty_device(arr.nbytes)
         t = srv.submit(d_in.data_ptr(), d_out.data_ptr(), len(arr))
-        assert srv.wait(t) == bs.OK
+        assert srv.wait(t, 60_000_000) == bs.OK
         torch.cuda.synchronize()
         outs.append(from_device(d_out[:arr.nbytes], bs.NP_DTYPES[dtype]))
     return outs
@@ -66,7 +66,7 @@ def sort_in_mix(srv, dtype, reqs, threads=3):
     for x in th:
         x.join()
     for t in tickets:
-        assert srv.wait(t) == bs.OK
+        assert srv.wait(t, 60_000_000) == bs.OK
     torch.cuda.synchronize()
     return [from_device(d_out[i][:reqs[i].nbytes], bs.NP_DTYPES[dtype]) for i in range(len(reqs))]
 
@@ -122,7 +122,7 @@ def test_host_memory_requests_pinned_and_pageable():
             tickets.append(srv.submit(sp, dp, len(arr), bs.MEM_HOST))
             outs.append(keep)
         for t in tickets:
-            assert srv.wait(t) == bs.OK
+            assert srv.wait(t, 60_000_000) == bs.OK
     for arr, (_, dst) in zip(reqs, outs):
         got = dst.numpy().view(bs.NP_DTYPES[dtype]) if isinstance(dst, torch.Tensor) else dst
         assert np.array_equal(got, expected_one(dtype, 0, arr))
@@ -155,6 +155,6 @@ def test_zero_length_and_queue_state():
     with bs.Server(dtype, budget_bytes=1 << 20) as srv:
         t = srv.submit(0, 0, 0)
         assert srv.poll(t)[0] == bs.REQ_DONE
-        assert srv.wait(t) == bs.OK
+        assert srv.wait(t, 60_000_000) == bs.OK
         srv.drain(5_000_000)
         assert srv.stats().queued == 0
