@@ -57,6 +57,11 @@ class Tile(ctypes.Structure):
                     self.log2_ctas)
 
 
+class TileInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("registers_per_thread", "local_bytes_per_thread", "shared_bytes",
+                                              "cta_threads", "active_ctas_per_sm", "working", "arrays_per_cta")]
+
+
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("dtype", ctypes.c_int), ("flags", ctypes.c_uint32),
                 ("budget_bytes", ctypes.c_int64), ("max_inflight", ctypes.c_int32), ("max_batch", ctypes.c_int32),
@@ -90,6 +95,8 @@ _SIGNATURES = {
     "b200s_tile_count": (ctypes.c_int32, [ctypes.c_int, ctypes.c_uint32]),
     "b200s_tile_get": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.c_int32, ctypes.POINTER(Tile)]),
     "b200s_default_tile": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.c_int32, ctypes.POINTER(Tile)]),
+    "b200s_tile_info_get": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(Tile), ctypes.c_int32,
+                                           ctypes.POINTER(TileInfo)]),
     "b200s_load_tile_table": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32)]),
     "b200s_sort_packed": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                          ctypes.c_int64, ctypes.c_uint32, ctypes.POINTER(Tile),
@@ -176,6 +183,14 @@ def default_tile(dtype, n, flags=0):
     t = Tile()
     check(lib().b200s_default_tile(dtype, flags, n, ctypes.byref(t)))
     return t
+
+
+def tile_info(dtype, n, flags=0, tile=None):
+    """Registers, local memory, shared memory and residency of the kernel for length n."""
+    out = TileInfo()
+    check(lib().b200s_tile_info_get(dtype, flags, ctypes.byref(tile) if tile is not None else None, n,
+                                    ctypes.byref(out)))
+    return out
 
 
 def load_tile_table(path):

@@ -1,6 +1,9 @@
 // CUB BlockMergeSort baseline (NOT part of the product; built into its own
 // library, libb200sort_cub.so, and only timed beside the product).
 //
+// Also Thrust's per-segment loop (one thrust::sort call per array, as the
+// reference's thrust_segment_loop method times it, bench.cu:575-585).
+//
 // One CTA per array of a packed batch, in place: BlockLoad (warp transpose,
 // maximum-key default) -> BlockMergeSort(valid_items, maximum) -> BlockStore,
 // the library's standard block-sort sequence, as the reference times it
@@ -9,6 +12,9 @@
 #include <cub/block/block_load.cuh>
 #include <cub/block/block_merge_sort.cuh>
 #include <cub/block/block_store.cuh>
+#include <thrust/device_ptr.h>
+#include <thrust/execution_policy.h>
+#include <thrust/sort.h>
 
 #include <climits>
 #include <cstdint>
@@ -22,6 +28,9 @@ struct Rec {
 
 struct LessI32 {
     __device__ bool operator()(const int& a, const int& b) const { return a < b; }
+};
+struct KeyLessRec {
+    __host__ __device__ bool operator()(const Rec& a, const Rec& b) const { return a.key < b.key; }
 };
 struct LessRec {
     __device__ bool operator()(const Rec& a, const Rec& b) const {
@@ -90,5 +99,22 @@ int cub_block_merge_sort(int dtype, void* d, int n, int arrays, int working, int
     if (dtype == 0) return by_working<int, LessI32, 32>(working, threads, d, n, arrays, st);
     if (dtype == 1) return by_working<Rec, LessRec, 32>(working, threads, d, n, arrays, st);
     return 1;
+}
+
+// One thrust::sort per array on `stream`, in place (records by key only).
+int thrust_segment_sort(int dtype, void* d, int n, int arrays, void* stream) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (int a = 0; a < arrays; ++a) {
+        if (dtype == 0) {
+            int* p = static_cast<int*>(d) + size_t(a) * n;
+            thrust::sort(thrust::cuda::par.on(st), p, p + n);
+        } else if (dtype == 1) {
+            Rec* p = static_cast<Rec*>(d) + size_t(a) * n;
+            thrust::sort(thrust::cuda::par.on(st), p, p + n, KeyLessRec{});
+        } else {
+            return 1;
+        }
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 }

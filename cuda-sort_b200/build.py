@@ -18,6 +18,7 @@ BASELINES = os.path.join(HERE, "baselines")
 CUB_LIB = os.path.join(HERE, "libb200sort_cub.so")
 HARNESS = os.path.join(HERE, "harness")
 LOADGEN_LIB = os.path.join(HERE, "libb200sort_loadgen.so")
+BENCH_CLI = os.path.join(HERE, "b200sort_bench")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -78,8 +79,9 @@ def build(verbose=False, extra=None, jobs=None):
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
     build_cub_baseline()
     build_loadgen()
+    build_bench_cli()
     if verbose:
-        print("built", LIB, CUB_LIB, LOADGEN_LIB)
+        print("built", LIB, CUB_LIB, LOADGEN_LIB, BENCH_CLI)
     return LIB
 
 
@@ -107,6 +109,20 @@ def build_loadgen():
     if r.returncode != 0:
         raise RuntimeError("load generator build failed:\n" + r.stdout + r.stderr)
     return LOADGEN_LIB
+
+
+def build_bench_cli():
+    """b200sort_bench: the reference's bench command line and CSV over the library and the baselines."""
+    src = os.path.join(HARNESS, "bench_cli.cu")
+    deps = [src, LIB, CUB_LIB, os.path.join(ROOT, "include", "b200sort.h")]
+    if os.path.exists(BENCH_CLI) and os.path.getmtime(BENCH_CLI) >= max(os.path.getmtime(d) for d in deps):
+        return BENCH_CLI
+    cmd = [NVCC] + ARCH + ["-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), src, "-o", BENCH_CLI,
+                           "-L" + HERE, "-lb200sort", "-l:libb200sort_cub.so", "-Xlinker", "-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("bench CLI build failed:\n" + r.stdout + r.stderr)
+    return BENCH_CLI
 
 
 if __name__ == "__main__":

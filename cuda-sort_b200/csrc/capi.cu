@@ -352,6 +352,43 @@ b200s_status b200s_default_tile(b200s_dtype dtype, uint32_t flags, int32_t n, b2
     return B200S_OK;
 }
 
+b200s_status b200s_tile_info_get(b200s_dtype dtype, uint32_t flags, const b200s_tile* tile, int32_t n,
+                                 b200s_tile_info* out) {
+    if (!valid_dtype(dtype) || !out || n < 0)
+        return set_error(B200S_ERR_INVALID_ARGUMENT, "b200s_tile_info_get: bad argument");
+    b200s_status st;
+    int persistent = 0;
+    const int idx = select_entry(dtype, flags, std::max(1, n), tile, &st, &persistent);
+    if (idx < 0) return st;
+    const KernelEntry& e = registry()[size_t(idx)];
+    cudaFuncAttributes a = {};
+    const cudaError_t ce = e.attrs(&a);
+    if (ce != cudaSuccess) return cuda_error(ce, "cudaFuncGetAttributes");
+    int dev = 0, sm_threads = 2048, sm_regs = 65536, sm_smem = 228 * 1024, sm_blocks = 32;
+    if (cudaGetDevice(&dev) == cudaSuccess) {
+        cudaDeviceGetAttribute(&sm_threads, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+        cudaDeviceGetAttribute(&sm_regs, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&sm_blocks, cudaDevAttrMaxBlocksPerMultiprocessor, dev);
+    }
+    // residency limits: threads, registers (allocated per warp in units of
+    // 256), shared memory (plus 1 KB reserved per CTA), CTA slots
+    const int warps = (e.cta + 31) / 32;
+    const int regs_per_warp = ((a.numRegs * 32 + 255) / 256) * 256;
+    const size_t smem = size_t(a.sharedSizeBytes) + e.smem + 1024;
+    int active = std::min(sm_blocks, sm_threads / std::max(1, e.cta));
+    if (regs_per_warp > 0) active = std::min(active, sm_regs / (regs_per_warp * warps));
+    active = std::min<int>(active, int(size_t(sm_smem) / smem));
+    out->registers_per_thread = a.numRegs;
+    out->local_bytes_per_thread = int32_t(a.localSizeBytes);
+    out->shared_bytes = int32_t(a.sharedSizeBytes + e.smem);
+    out->cta_threads = e.cta;
+    out->active_ctas_per_sm = active;
+    out->working = int32_t(1) << e.log2w;
+    out->arrays_per_cta = e.lc >= 0 ? 0 : e.apc;
+    return B200S_OK;
+}
+
 b200s_status b200s_load_tile_table(const char* path, int32_t* applied) {
     if (!path) return set_error(B200S_ERR_INVALID_ARGUMENT, "b200s_load_tile_table: null path");
     TableRows rows;

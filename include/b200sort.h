@@ -101,6 +101,21 @@ int32_t b200s_tile_count(b200s_dtype dtype, uint32_t flags);
 b200s_status b200s_tile_get(b200s_dtype dtype, uint32_t flags, int32_t index, b200s_tile* out);
 /* Tile the library uses for arrays of length n when the caller passes none. */
 b200s_status b200s_default_tile(b200s_dtype dtype, uint32_t flags, int32_t n, b200s_tile* out);
+/* Resources of the kernel that sorts arrays of length n with `tile` (NULL:
+ * the default tile), as the reference's bench reports them for its kernels
+ * (bench.cu:425-440): registers and local memory per thread, shared memory
+ * per CTA, threads per CTA, and CTAs resident per SM (computed from those). */
+typedef struct b200s_tile_info {
+    int32_t registers_per_thread;
+    int32_t local_bytes_per_thread;
+    int32_t shared_bytes;
+    int32_t cta_threads;
+    int32_t active_ctas_per_sm;
+    int32_t working;        /* working length W of the tile */
+    int32_t arrays_per_cta; /* 0 for cluster tiles (several CTAs per array) */
+} b200s_tile_info;
+b200s_status b200s_tile_info_get(b200s_dtype dtype, uint32_t flags, const b200s_tile* tile, int32_t n,
+                                 b200s_tile_info* out);
 /* Replace rows of the default tile table from a CSV file; '#' starts a
  * comment.  Packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps
  * [,persistent].  Ragged rows: r,dtype,flags,log2_w,family (0: the larger
