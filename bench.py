@@ -83,6 +83,11 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="ragged workloads: skip the per-length comparison")
     ap.add_argument("--preroll", type=float, default=1.5,
                     help="seconds of untimed sorting before the timed region, so clocks settle")
+    ap.add_argument("--form", default="table", choices=["table", "0", "1", "2"],
+                    help="packed workloads: launch form of the tabled tile (0 one-shot, 1 register prefetch, "
+                         "2 TMA pipeline); 'table' uses the tile table's choice")
+    ap.add_argument("--tile", default=None, help="packed workloads: tile shape log2_items,log2_lanes,log2_warps "
+                                                  "instead of the table's")
     ap.add_argument("--duration", type=float, default=2.0, help="serving: seconds per rate point")
     ap.add_argument("--rates", default="1e4,3e4,1e5,3e5,1e6", help="serving: Poisson arrival rates (req/s)")
     return ap.parse_args()
@@ -365,16 +370,27 @@ def run_gpu(args, wl):
         d_in = [host.to(ctx.dev) for _ in range(sets)]
         d_out = [torch.empty_like(d_in[0]) for _ in range(sets)]
 
+        tile = None
+        if args.form != "table" or args.tile:
+            t = bs.default_tile(dtype, n, flags)
+            shape = [int(x) for x in args.tile.split(",")] if args.tile else [t.log2_items, t.log2_lanes, t.log2_warps]
+            form = t.persistent if args.form == "table" else int(args.form)
+            tile = bs.Tile(shape[0], shape[1], shape[2], 0, form, 0 if args.tile else t.log2_ctas)
+        eff = tile if tile is not None else bs.default_tile(dtype, n, flags)
+        extra["tile"] = repr(eff)
+        tma_ok = (n * eb) % 128 == 0 and n * eb // 128 <= 256 and eff.log2_warps == 0 and eff.log2_ctas == 0
+        form = eff.persistent if (eff.persistent != 2 or tma_ok) else 0
+
         def step(i):
             k = i % sets
-            bs.sort_packed(dtype, d_in[k].data_ptr(), d_out[k].data_ptr(), n, arrays, flags, None, ctx.sh)
+            bs.sort_packed(dtype, d_in[k].data_ptr(), d_out[k].data_ptr(), n, arrays, flags, tile, ctx.sh)
 
         ms_step, clocks = timed_region(ctx, step, args)
         got = d_out[(args.steps - 1) % sets].cpu().numpy().view(bs.NP_DTYPES[dtype])
         keys_in = data if dtype in (bs.I32, bs.U64) else data["key"]
         keys_out = got if dtype in (bs.I32, bs.U64) else got["key"]
         verified = bool(np.array_equal(keys_out.reshape(arrays, n), np.sort(keys_in.reshape(arrays, n), axis=1)))
-        kernel = "k_sort_packed"
+        kernel = {0: "k_sort_packed", 1: "k_sort_packed_pf", 2: "k_sort_packed_tma"}[form]
         launches = args.steps
     else:
         arrays = wl["arrays"]

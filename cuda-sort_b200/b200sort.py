@@ -48,18 +48,23 @@ class Tile(ctypes.Structure):
         return (self.log2_items, self.log2_lanes, self.log2_warps, self.log2_ctas)
 
     def __repr__(self):
-        return "Tile(K=%d, lanes=%d, warps=%d, ctas=%d, cta=%d%s)" % (
+        return "Tile(K=%d, lanes=%d, warps=%d, ctas=%d, cta=%d, form=%d)" % (
             1 << self.log2_items, 1 << self.log2_lanes, 1 << self.log2_warps, 1 << self.log2_ctas,
-            self.cta_threads, ", persistent" if self.persistent else "")
+            self.cta_threads, self.persistent)
 
     def with_persistent(self, on=True):
         return Tile(self.log2_items, self.log2_lanes, self.log2_warps, self.cta_threads, 1 if on else 0,
                     self.log2_ctas)
 
+    def with_form(self, form):
+        """The same shape with launch form 0 (one-shot), 1 (register prefetch) or 2 (TMA pipeline)."""
+        return Tile(self.log2_items, self.log2_lanes, self.log2_warps, self.cta_threads, form, self.log2_ctas)
+
 
 class TileInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int32) for n in ("registers_per_thread", "local_bytes_per_thread", "shared_bytes",
-                                              "cta_threads", "active_ctas_per_sm", "working", "arrays_per_cta")]
+                                              "cta_threads", "active_ctas_per_sm", "working", "arrays_per_cta",
+                                              "tma_form")]
 
 
 class ServerConfig(ctypes.Structure):

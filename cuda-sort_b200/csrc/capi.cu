@@ -213,7 +213,10 @@ b200s_status parse_table_file(const char* path, TableRows* out) {
         if (idx < 0 || registry()[size_t(idx)].log2w < w)
             return set_error(B200S_ERR_UNSUPPORTED,
                              "tile table line " + std::to_string(lineno) + ": tile not compiled or too short");
-        out->packed.push_back({d * 2 + stable, w, idx, pers ? 1 : 0});
+        if (pers < 0 || pers > 2)
+            return set_error(B200S_ERR_INVALID_ARGUMENT,
+                             "tile table line " + std::to_string(lineno) + ": launch form must be 0, 1 or 2");
+        out->packed.push_back({d * 2 + stable, w, idx, pers});
     }
     return B200S_OK;
 }
@@ -246,10 +249,33 @@ int lookup_default_entry(int dtype, int stable, long long n, int* persistent) {
 
 void set_ragged_family(int dtype, int stable, int log2w, int family);
 
-// Launch the packed kernel of registry entry `idx`.
+// The TMA-pipelined kernel for registry entry e and this batch, or null when
+// the batch does not meet its requirements: whole 128-byte rows per array (at
+// most 256), 16-byte aligned buffers, int32-addressable array indices.
+const TmaEntry* tma_for(const KernelEntry& e, const void* in, const void* out, int n, long long arrays) {
+    if (e.lw != 0 || e.lc >= 0) return nullptr;
+    const long long bytes = (long long)n * (long long)elem_bytes(e.dtype);
+    if (bytes % 128 != 0 || bytes / 128 > 256 || arrays > 0x7fffffffLL) return nullptr;
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) return nullptr;
+    for (const TmaEntry& t : tma_registry())
+        if (t.dtype == e.dtype && t.stable == e.stable && t.lk == e.lk && t.lg == e.lg) return &t;
+    return nullptr;
+}
+
+// Launch the packed kernel of registry entry `idx`: form 0 one-shot, 1
+// persistent with register prefetch, 2 persistent TMA pipeline (form 0 when
+// the batch does not qualify).
 b200s_status launch_packed(int idx, int persistent, const void* in, void* out, int n,
                            long long arrays, cudaStream_t st) {
     const KernelEntry& e = registry()[size_t(idx)];
+    if (persistent == 2) {
+        if (const TmaEntry* t = tma_for(e, in, out, n, arrays)) {
+            const cudaError_t err = t->launch(in, out, n, arrays, st);
+            if (err != cudaSuccess) return cuda_error(err, "TMA sort kernel launch");
+            return B200S_OK;
+        }
+        persistent = 0;
+    }
     long long grid = (arrays + e.apc - 1) / e.apc;
     grid = std::min<long long>(grid, 0x7fffffffLL);
     cudaError_t err = persistent ? e.launch_pf(in, out, n, arrays, grid, st)
@@ -264,7 +290,7 @@ int select_entry(int dtype, uint32_t flags, long long n, const b200s_tile* tile,
     int idx;
     *persistent = 0;
     if (tile) {
-        *persistent = tile->persistent ? 1 : 0;
+        *persistent = tile->persistent < 0 ? 0 : (tile->persistent > 2 ? 2 : tile->persistent);
         idx = lookup_tile(dtype, stable, *tile);
         if (idx < 0) {
             *st = set_error(B200S_ERR_UNSUPPORTED, "no compiled kernel for the requested tile");
@@ -386,6 +412,16 @@ b200s_status b200s_tile_info_get(b200s_dtype dtype, uint32_t flags, const b200s_
     out->active_ctas_per_sm = active;
     out->working = int32_t(1) << e.log2w;
     out->arrays_per_cta = e.lc >= 0 ? 0 : e.apc;
+    static const char aligned[16] = {};  // any 16-byte aligned address stands for the buffers
+    out->tma_form = tma_for(e, aligned, aligned, std::max(1, n), 1) ? 1 : 0;
+    return B200S_OK;
+}
+
+b200s_status b200s_tma_timeouts(int64_t* count) {
+    if (!count) return set_error(B200S_ERR_INVALID_ARGUMENT, "null count");
+    const int64_t v = tma_timeouts();
+    if (v < 0) return set_error(B200S_ERR_CUDA, "reading the TMA status word failed");
+    *count = v;
     return B200S_OK;
 }
 

@@ -59,18 +59,80 @@ __device__ __forceinline__ void cluster_layer(typename E::Reg (&v)[S::K], const 
     }
 }
 
+// Cross-CTA layer with a run-time CTA mask cm: the partner of (rank, t, q)
+// is (rank ^ cm, t ^ TM, q ^ RM); a reflection flips every lower bit (RM, TM
+// all ones), a merge only the CTA bit.
+template <class E, class S, unsigned RM, unsigned TM>
+__device__ __forceinline__ void cta_layer_rt(typename E::Reg (&v)[S::K], const int t, const int rank, const int cm,
+                                             const bool upper, typename E::Reg* cur) {
+    using R = typename E::Reg;
+    cg::cluster_group cluster = cg::this_cluster();
+    sfor<0, S::K>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        cur[q * S::TPA + t] = v[q];
+    });
+    cluster.sync();
+    const R* remote = cluster.map_shared_rank(cur, rank ^ cm);
+    sfor<0, S::K>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        const R b = remote[(q ^ int(RM)) * S::TPA + (t ^ int(TM))];
+        v[q] = E::pick(v[q], b, upper);
+    });
+    cluster.sync();
+}
+
+// The cluster network with the stages above one CTA as a run-time loop
+// (one copy of their code), for elements whose unrolled network would not
+// fit the instruction cache.
+template <class E, class S, int LC, bool SB>
+__device__ __forceinline__ void cluster_network_compact(typename E::Reg (&v)[S::K], const int t, const int rank,
+                                                        typename E::Reg*& cur, typename E::Reg*& nxt) {
+    constexpr int LOCAL = S::LOGW;
+    // stages inside one CTA
+    if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{});
+    else network<E, S>(v, t, cur, nxt, CtaBarrier{});
+#pragma unroll 1
+    for (int st = LOCAL; st < LOCAL + LC; ++st) {
+        cta_layer_rt<E, S, unsigned(S::K - 1), unsigned(S::TPA - 1)>(v, t, rank, (2 << (st - LOCAL)) - 1,
+                                                                        (rank >> (st - LOCAL)) & 1, cur);
+#pragma unroll 1
+        for (int j = st - 1; j >= LOCAL; --j)
+            cta_layer_rt<E, S, 0u, 0u>(v, t, rank, 1 << (j - LOCAL), (rank >> (j - LOCAL)) & 1, cur);
+        // merges inside the CTA: warp and lane bits at run time, then registers
+#pragma unroll 1
+        for (int j = LOCAL - 1; j >= S::LK; --j) {
+            if constexpr (SB) cross_layer_rt<E, S, 0u>(v, t, j, cur, nxt, CtaBarrierSingle{});
+            else cross_layer_rt<E, S, 0u>(v, t, j, cur, nxt, CtaBarrier{});
+        }
+        sfor<0, S::LK>([&](auto jc) {
+            constexpr int j = S::LK - 1 - decltype(jc)::value;
+            layer<E, S, (1u << j)>(v, t, cur, nxt, CtaBarrier{});
+        });
+    }
+}
+
+// Element types may opt out of the compact form in clusters only.
+template <class E, class = void>
+struct compact_cluster : std::integral_constant<bool, E::kCompact> {};
+template <class E>
+struct compact_cluster<E, std::void_t<decltype(E::kCompactCluster)>> : std::integral_constant<bool, E::kCompactCluster> {};
+
 template <class E, class S, int LC, bool SB>
 __device__ __forceinline__ void cluster_network(typename E::Reg (&v)[S::K], const int t, const int rank,
                                                 typename E::Reg*& cur, typename E::Reg*& nxt) {
-    constexpr int LOGW = S::LOGW + LC;
-    sfor<0, LOGW>([&](auto sc) {
-        constexpr int ST = decltype(sc)::value;
-        cluster_layer<E, S, LC, (2u << ST) - 1u, SB>(v, t, rank, cur, nxt);
-        sfor<0, ST>([&](auto jc) {
-            constexpr int j = ST - 1 - decltype(jc)::value;
-            cluster_layer<E, S, LC, (1u << j), SB>(v, t, rank, cur, nxt);
+    if constexpr (use_compact<E, S>() && compact_cluster<E>::value) {
+        cluster_network_compact<E, S, LC, SB>(v, t, rank, cur, nxt);
+    } else {
+        constexpr int LOGW = S::LOGW + LC;
+        sfor<0, LOGW>([&](auto sc) {
+            constexpr int ST = decltype(sc)::value;
+            cluster_layer<E, S, LC, (2u << ST) - 1u, SB>(v, t, rank, cur, nxt);
+            sfor<0, ST>([&](auto jc) {
+                constexpr int j = ST - 1 - decltype(jc)::value;
+                cluster_layer<E, S, LC, (1u << j), SB>(v, t, rank, cur, nxt);
+            });
         });
-    });
+    }
 }
 
 // One cluster per array, clusters striding over the batch.  Packed batches

@@ -101,6 +101,7 @@ struct ElemI32 {
     using Mem = int32_t;
     using Reg = int32_t;
     static constexpr bool kStable = false;
+    static constexpr bool kCompact = false;
     static __device__ __forceinline__ Reg pad() { return INT32_MAX; }
     static __device__ __forceinline__ Reg from_mem(Mem m, int) { return m; }
     static __device__ __forceinline__ Mem to_mem(Reg r) { return r; }
@@ -124,6 +125,7 @@ struct ElemU64 {
     using Mem = uint64_t;
     using Reg = uint64_t;
     static constexpr bool kStable = false;
+    static constexpr bool kCompact = true;
     static __device__ __forceinline__ Reg pad() { return UINT64_MAX; }
     static __device__ __forceinline__ Reg from_mem(Mem m, int) { return m; }
     static __device__ __forceinline__ Mem to_mem(Reg r) { return r; }
@@ -149,6 +151,7 @@ struct ElemRecI32 {
     using Mem = RecI32;
     using Reg = RegRecI32;
     static constexpr bool kStable = false;
+    static constexpr bool kCompact = true;
     static __device__ __forceinline__ Reg pad() { return Reg{INT32_MAX, INT32_MAX}; }
     static __device__ __forceinline__ Reg from_mem(Mem m, int) { return Reg{m.key, m.data}; }
     static __device__ __forceinline__ Mem to_mem(Reg r) { return Mem{r.key, r.data}; }
@@ -180,6 +183,7 @@ struct ElemRecI32S {
     using Mem = RecI32;
     using Reg = RegRecI32S;
     static constexpr bool kStable = true;
+    static constexpr bool kCompact = true;
     static __device__ __forceinline__ Reg pad() { return Reg{INT32_MAX, INT32_MAX, INT32_MAX}; }
     static __device__ __forceinline__ Reg from_mem(Mem m, int pos) { return Reg{m.key, m.data, pos}; }
     static __device__ __forceinline__ Mem to_mem(Reg r) { return Mem{r.key, r.data}; }
@@ -210,6 +214,8 @@ struct ElemRecU64 {
     using Mem = RecU64;
     using Reg = RegRecU64;
     static constexpr bool kStable = false;
+    static constexpr bool kCompact = true;
+    static constexpr bool kCompactCluster = false;  // the cluster kernel spills more in the compact form
     static __device__ __forceinline__ Reg pad() { return Reg{UINT64_MAX, INT32_MAX}; }
     static __device__ __forceinline__ Reg from_mem(Mem m, int) { return Reg{m.key, m.data}; }
     static __device__ __forceinline__ Mem to_mem(Reg r) { return Mem{r.key, r.data, 0}; }
@@ -237,6 +243,7 @@ struct ElemRecU64S {
     using Mem = RecU64;
     using Reg = RegRecU64S;
     static constexpr bool kStable = true;
+    static constexpr bool kCompact = true;
     static __device__ __forceinline__ Reg pad() { return Reg{UINT64_MAX, INT32_MAX, INT32_MAX}; }
     static __device__ __forceinline__ Reg from_mem(Mem m, int pos) { return Reg{m.key, m.data, pos}; }
     static __device__ __forceinline__ Mem to_mem(Reg r) { return Mem{r.key, r.data, 0}; }

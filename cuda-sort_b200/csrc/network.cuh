@@ -151,12 +151,114 @@ __device__ __forceinline__ void stage(typename E::Reg (&v)[S::K], const int t,
     });
 }
 
+// ---- compact form ------------------------------------------------------------
+// The same layers with the lane / warp part of the partner mask known only at
+// run time, so that the stages whose span leaves the registers share one copy
+// of their code.  A cross-lane or cross-warp layer pairs (t, q) with
+// (t ^ tm, q ^ RM): RM is all register bits for a reflection and 0 for a
+// merge, whatever the stage.
+
+template <class E, class S, unsigned RM>
+__device__ __forceinline__ void lane_layer_rt(typename E::Reg (&v)[S::K], const int tm, const bool upper) {
+    using R = typename E::Reg;
+    if constexpr (RM == 0) {
+        sfor<0, S::K>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            const R b = E::shfl(v[q], tm);
+            v[q] = E::pick(v[q], b, upper);
+        });
+    } else {
+        sfor<0, S::K>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr int p = q ^ int(RM);
+            if constexpr (q < p) {
+                const R bq = E::shfl(v[p], tm);
+                const R bp = E::shfl(v[q], tm);
+                v[q] = E::pick(v[q], bq, upper);
+                v[p] = E::pick(v[p], bp, upper);
+            }
+        });
+    }
+}
+
+template <class E, class S, unsigned RM, class Bar>
+__device__ __forceinline__ void warp_layer_rt(typename E::Reg (&v)[S::K], const int t, const int tm,
+                                              const bool upper, typename E::Reg*& cur, typename E::Reg*& nxt,
+                                              const Bar& bar) {
+    using R = typename E::Reg;
+    sfor<0, S::K>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        cur[q * S::TPA + t] = v[q];
+    });
+    bar();
+    sfor<0, S::K>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        const R b = cur[(q ^ int(RM)) * S::TPA + (t ^ tm)];
+        v[q] = E::pick(v[q], b, upper);
+    });
+    if constexpr (single_buffer<Bar>::value) {
+        bar();
+    } else {
+        R* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+    }
+}
+
+// Layer with partner mask bit j >= LK (runtime j); reflection when RM != 0.
+template <class E, class S, unsigned RM, class Bar>
+__device__ __forceinline__ void cross_layer_rt(typename E::Reg (&v)[S::K], const int t, const int j,
+                                               typename E::Reg*& cur, typename E::Reg*& nxt, const Bar& bar) {
+    const int tm = RM ? (2 << (j - S::LK)) - 1 : 1 << (j - S::LK);
+    const bool upper = (t >> (j - S::LK)) & 1;
+    if constexpr (S::LW == 0) {
+        lane_layer_rt<E, S, RM>(v, tm, upper);
+    } else {
+        if (j < S::LK + S::LG) lane_layer_rt<E, S, RM>(v, tm, upper);
+        else warp_layer_rt<E, S, RM>(v, t, tm, upper, cur, nxt, bar);
+    }
+}
+
+template <class E, class S, class Bar>
+__device__ __forceinline__ void network_compact(typename E::Reg (&v)[S::K], const int t, typename E::Reg*& cur,
+                                                typename E::Reg*& nxt, const Bar& bar) {
+    constexpr int LK = S::LK;
+    // stages inside the registers: unrolled
+    sfor<0, (LK < S::LOGW ? LK : S::LOGW)>([&](auto sc) { stage<E, S, decltype(sc)::value>(v, t, cur, nxt, bar); });
+#pragma unroll 1
+    for (int st = LK; st < S::LOGW; ++st) {
+        cross_layer_rt<E, S, unsigned(S::K - 1)>(v, t, st, cur, nxt, bar);  // reflection
+#pragma unroll 1
+        for (int j = st - 1; j >= LK; --j) cross_layer_rt<E, S, 0u>(v, t, j, cur, nxt, bar);
+        // merges 2^(LK-1) .. 1 inside the registers
+        sfor<0, LK>([&](auto jc) {
+            constexpr int j = LK - 1 - decltype(jc)::value;
+            layer<E, S, (1u << j)>(v, t, cur, nxt, bar);
+        });
+    }
+}
+
+// The unrolled form is kept where its code stays small (a compare-exchange
+// of int32 keys is two instructions) or where the compact form's longer live
+// ranges make the compiler spill (uint64-key records: E::kCompact false);
+// the other element types take several instructions per compare-exchange and
+// their fully unrolled networks overflow the instruction cache, so they use
+// the compact form.
+template <class E, class S>
+constexpr bool use_compact() {
+    return E::kCompact && S::LOGW > S::LK;
+}
+
 // Sort the W-element tile held by the TPA threads of one array.
 template <class E, class S, class Bar = CtaBarrier>
 __device__ __forceinline__ void network(typename E::Reg (&v)[S::K], const int t,
                                         typename E::Reg*& cur, typename E::Reg*& nxt,
                                         const Bar& bar = Bar()) {
-    sfor<0, S::LOGW>([&](auto sc) { stage<E, S, decltype(sc)::value>(v, t, cur, nxt, bar); });
+    if constexpr (use_compact<E, S>()) {
+        network_compact<E, S>(v, t, cur, nxt, bar);
+    } else {
+        sfor<0, S::LOGW>([&](auto sc) { stage<E, S, decltype(sc)::value>(v, t, cur, nxt, bar); });
+    }
 }
 
 // ---- tile load / store --------------------------------------------------------

@@ -61,6 +61,16 @@ struct RaggedEntry {
     int (*resident_per_sm)();  // CTAs per SM (occupancy), 0 on error
 };
 
+// TMA-pipelined packed kernels (launch form 2) of single-warp-team tiles.
+struct TmaEntry {
+    int dtype;
+    int stable;
+    int lk, lg;
+    cudaError_t (*launch)(const void* in, void* out, int n, long long arrays, cudaStream_t stream);
+};
+const std::vector<TmaEntry>& tma_registry();
+int64_t tma_timeouts();  // CTAs of the TMA kernels that gave up waiting for a load
+
 void register_ragged_i32(std::vector<RaggedEntry>& out);
 void register_ragged_rec(std::vector<RaggedEntry>& out);
 void register_ragged_u64(std::vector<RaggedEntry>& out);

@@ -4,8 +4,8 @@ at first use from beside libb200sort.so).
   python cuda-sort_b200/tune_b200.py [--out PATH] [--reps R]
 
 For every element type, stable flag and working length W = 2^L it times each
-compiled single-CTA tile of that W in both launch forms (one slot per array /
-persistent with prefetch) on a full-length batch of about 4 M elements and
+compiled single-CTA tile of that W in each launch form (one slot per array /
+persistent with register prefetch / persistent TMA pipeline) on a full-length batch of about 4 M elements and
 keeps the fastest as the packed row.  For the ragged kernel it times, per
 bucket L, a batch whose lengths all fall in that bucket with the bucket's
 shape family A and with family B, and keeps the faster as the ragged row.
@@ -61,7 +61,10 @@ def tune_packed(dtype, flags, flush, reps, log):
         st = torch.cuda.current_stream().cuda_stream
         best = None
         for base in by_w[L]:
-            for tile in (base, base.with_persistent()):
+            forms = [base, base.with_persistent()]
+            if bs.tile_info(dtype, n, flags, base).tma_form:
+                forms.append(base.with_form(2))   # TMA pipeline, where compiled for this tile
+            for tile in forms:
                 us = timed(lambda t=tile: bs.sort_packed(dtype, d_in.data_ptr(), d_out.data_ptr(), n, arrays, flags,
                                                          t, st), flush, reps)
                 log("packed dtype=%d flags=%d W=%d %r: %.2f us" % (dtype, flags, n, tile, us))
@@ -126,7 +129,7 @@ def main():
         f.write("# device: %s; %s; library: %s\n" % (torch.cuda.get_device_name(),
                                                      datetime.datetime.now(datetime.timezone.utc).strftime(
                                                          "%Y-%m-%d %H:%M UTC"), bs.version()))
-        f.write("# packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps,persistent\n")
+        f.write("# packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps,form (0 one-shot, 1 prefetch, 2 TMA)\n")
         f.write("# ragged rows: r,dtype,flags,log2_w,family (0: larger per-thread tile, 1: smaller)\n")
         for ln in lines:
             f.write(ln + "\n")

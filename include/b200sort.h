@@ -82,8 +82,12 @@ typedef struct b200s_tile {
     int32_t log2_lanes;
     int32_t log2_warps;
     int32_t cta_threads; /* threads per CTA (output of the query functions) */
-    int32_t persistent;  /* 0: one launch slot per array group; 1: grid sized to the
-                            resident capacity, each group prefetching its next array */
+    int32_t persistent;  /* launch form. 0: one launch slot per array group; 1: grid sized
+                            to the resident capacity, each group prefetching its next array
+                            into registers; 2: persistent CTAs streaming chunks of arrays
+                            through shared memory with TMA loads and stores (used when every
+                            array is whole 128-byte rows, at most 256, and the buffers are
+                            16-byte aligned; form 0 otherwise) */
     int32_t log2_ctas;   /* CTAs per array: 0 for single-CTA tiles (cluster tiles of one
                             CTA exist only where no single-CTA tile of that shape does) */
 } b200s_tile;
@@ -113,12 +117,17 @@ typedef struct b200s_tile_info {
     int32_t active_ctas_per_sm;
     int32_t working;        /* working length W of the tile */
     int32_t arrays_per_cta; /* 0 for cluster tiles (several CTAs per array) */
+    int32_t tma_form;       /* 1 if launch form 2 runs a TMA kernel for this tile and n */
 } b200s_tile_info;
 b200s_status b200s_tile_info_get(b200s_dtype dtype, uint32_t flags, const b200s_tile* tile, int32_t n,
                                  b200s_tile_info* out);
+/* CTAs of the TMA-pipelined kernels on the current device that stopped
+ * waiting for a load after about a second (each left its chunk unsorted).
+ * Always 0 unless the device misbehaves; a cumulative count. */
+b200s_status b200s_tma_timeouts(int64_t* count);
 /* Replace rows of the default tile table from a CSV file; '#' starts a
  * comment.  Packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps
- * [,persistent].  Ragged rows: r,dtype,flags,log2_w,family (0: the larger
+ * [,form] (form: 0, 1 or 2 as b200s_tile.persistent).  Ragged rows: r,dtype,flags,log2_w,family (0: the larger
  * per-thread tile, 1: the smaller one), read by plans created afterwards.
  * Returns the number of rows applied in *applied. */
 b200s_status b200s_load_tile_table(const char* path, int32_t* applied);
