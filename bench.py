@@ -103,6 +103,41 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
 
 
+def layer_counts(lk, lg, lw, lc=0):
+    """Comparator layers of the reflection network by where the partner lives:
+    (registers, lanes, warps through shared memory, cluster CTAs)."""
+    counts = [0, 0, 0, 0]
+    logw = lk + lg + lw + lc
+    for st in range(logw):
+        for hb in [st] + list(range(st - 1, -1, -1)):
+            counts[0 if hb < lk else 1 if hb < lk + lg else 2 if hb < lk + lg + lw else 3] += 1
+    return counts
+
+
+# ALU instructions per element and layer: int32 keys take one min or max per
+# element inside a thread and both (one kept per lane) across threads; records
+# take a compare and four selects per pair inside a thread and about five
+# instructions per element across threads.
+ALU_PER_ELEM = {bs.I32: (1.0, 2.0), bs.I32_I32: (2.5, 5.0), bs.U64: (2.5, 5.0), bs.U64_I32: (2.5, 5.0)}
+
+
+def alu_roofline(dtype, tile, elements, seconds, sm_mhz):
+    """Integer-ALU bound of the network: modelled instructions per element x
+    element slots over the B200's ALU rate (16 lanes per clock per SM
+    sub-partition, 4 per SM, 148 SMs)."""
+    reg, lane, warp, cta = layer_counts(tile.log2_items, tile.log2_lanes, tile.log2_warps, tile.log2_ctas)
+    inside, across = ALU_PER_ELEM[dtype]
+    per_elem = reg * inside + (lane + warp + cta) * across
+    sms = 148
+    mhz = sm_mhz or 1965.0
+    peak = 64 * sms * mhz * 1e6           # ALU lane-instructions per second
+    achieved = per_elem * elements / seconds
+    return {"ops_per_element": per_elem, "layers": {"registers": reg, "lanes": lane, "warps": warp, "ctas": cta},
+            "achieved_tops": achieved / 1e12, "peak_tops": peak / 1e12, "frac": achieved / peak,
+            "sm_mhz": mhz, "model": "int32: 1 ALU op per element per in-thread layer, 2 across threads; "
+                                    "records: 2.5 and 5 (compare + selects)"}
+
+
 def traffic_for(workload):
     """DRAM bytes per launch of the sort kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "traffic.txt")
@@ -432,6 +467,9 @@ def run_gpu(args, wl):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "peak_source": peak_src, "traffic": traffic_for(args.workload),
                 "algorithmic_bytes_per_launch": algo_bytes, "kernel": kernel, "launch_us": ms_step * 1e3}
+    if wl["kind"] == "packed":
+        w = 1 << (eff.log2_items + eff.log2_lanes + eff.log2_warps + eff.log2_ctas)
+        roofline["alu"] = alu_roofline(dtype, eff, wl["arrays"] * w, ms_step * 1e-3, clocks.get("sm_mhz"))
 
     e2e = None
     if not args.no_e2e:

@@ -14,7 +14,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libb200sort.so")
+# B200SORT_LIB names another build of the library (for example an experimental
+# one); its tile table is read from tune/b200_table.csv beside it.
+LIB_PATH = os.environ.get("B200SORT_LIB", os.path.join(HERE, "libb200sort.so"))
 
 I32, I32_I32, U64, U64_I32 = 0, 1, 2, 3
 DTYPES = {"i32": I32, "i32_i32": I32_I32, "u64": U64, "u64_i32": U64_I32}

@@ -111,16 +111,10 @@ __device__ __forceinline__ void cluster_network_compact(typename E::Reg (&v)[S::
     }
 }
 
-// Element types may opt out of the compact form in clusters only.
-template <class E, class = void>
-struct compact_cluster : std::integral_constant<bool, E::kCompact> {};
-template <class E>
-struct compact_cluster<E, std::void_t<decltype(E::kCompactCluster)>> : std::integral_constant<bool, E::kCompactCluster> {};
-
 template <class E, class S, int LC, bool SB>
 __device__ __forceinline__ void cluster_network(typename E::Reg (&v)[S::K], const int t, const int rank,
                                                 typename E::Reg*& cur, typename E::Reg*& nxt) {
-    if constexpr (use_compact<E, S>() && compact_cluster<E>::value) {
+    if constexpr (use_compact<E, S>()) {
         cluster_network_compact<E, S, LC, SB>(v, t, rank, cur, nxt);
     } else {
         constexpr int LOGW = S::LOGW + LC;

@@ -196,12 +196,20 @@ struct ElemRecI32S {
     static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
         const Reg a = lo, b = hi;
         const bool sw = lt(b, a);
-        lo = sw ? b : a;
-        hi = sw ? a : b;
+        lo.key = sw ? b.key : a.key;
+        lo.data = sw ? b.data : a.data;
+        lo.pos = sw ? b.pos : a.pos;
+        hi.key = sw ? a.key : b.key;
+        hi.data = sw ? a.data : b.data;
+        hi.pos = sw ? a.pos : b.pos;
     }
     static __device__ __forceinline__ Reg pick(Reg own, Reg other, bool upper) {
         const bool take = upper ? lt(own, other) : lt(other, own);
-        return take ? other : own;
+        Reg r;
+        r.key = take ? other.key : own.key;
+        r.data = take ? other.data : own.data;
+        r.pos = take ? other.pos : own.pos;
+        return r;
     }
 };
 
@@ -215,22 +223,28 @@ struct ElemRecU64 {
     using Reg = RegRecU64;
     static constexpr bool kStable = false;
     static constexpr bool kCompact = true;
-    static constexpr bool kCompactCluster = false;  // the cluster kernel spills more in the compact form
     static __device__ __forceinline__ Reg pad() { return Reg{UINT64_MAX, INT32_MAX}; }
     static __device__ __forceinline__ Reg from_mem(Mem m, int) { return Reg{m.key, m.data}; }
     static __device__ __forceinline__ Mem to_mem(Reg r) { return Mem{r.key, r.data, 0}; }
     static __device__ __forceinline__ Reg shfl(Reg v, int m) {
         return Reg{shfl_x(v.key, m), shfl_x(v.data, m)};
     }
+    // Field by field: whole-struct selects of this padded register record
+    // made the compiler spill in the large tiles.
     static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
         const Reg a = lo, b = hi;
         const bool sw = b.key < a.key;
-        lo = sw ? b : a;
-        hi = sw ? a : b;
+        lo.key = sw ? b.key : a.key;
+        lo.data = sw ? b.data : a.data;
+        hi.key = sw ? a.key : b.key;
+        hi.data = sw ? a.data : b.data;
     }
     static __device__ __forceinline__ Reg pick(Reg own, Reg other, bool upper) {
         const bool take = upper ? (own.key < other.key) : (other.key < own.key);
-        return take ? other : own;
+        Reg r;
+        r.key = take ? other.key : own.key;
+        r.data = take ? other.data : own.data;
+        return r;
     }
 };
 
@@ -256,12 +270,20 @@ struct ElemRecU64S {
     static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
         const Reg a = lo, b = hi;
         const bool sw = lt(b, a);
-        lo = sw ? b : a;
-        hi = sw ? a : b;
+        lo.key = sw ? b.key : a.key;
+        lo.data = sw ? b.data : a.data;
+        lo.pos = sw ? b.pos : a.pos;
+        hi.key = sw ? a.key : b.key;
+        hi.data = sw ? a.data : b.data;
+        hi.pos = sw ? a.pos : b.pos;
     }
     static __device__ __forceinline__ Reg pick(Reg own, Reg other, bool upper) {
         const bool take = upper ? lt(own, other) : lt(other, own);
-        return take ? other : own;
+        Reg r;
+        r.key = take ? other.key : own.key;
+        r.data = take ? other.data : own.data;
+        r.pos = take ? other.pos : own.pos;
+        return r;
     }
 };
 

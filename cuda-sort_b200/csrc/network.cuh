@@ -239,11 +239,10 @@ __device__ __forceinline__ void network_compact(typename E::Reg (&v)[S::K], cons
 }
 
 // The unrolled form is kept where its code stays small (a compare-exchange
-// of int32 keys is two instructions) or where the compact form's longer live
-// ranges make the compiler spill (uint64-key records: E::kCompact false);
-// the other element types take several instructions per compare-exchange and
-// their fully unrolled networks overflow the instruction cache, so they use
-// the compact form.
+// of int32 keys is two instructions, E::kCompact false); the other element
+// types take several instructions per compare-exchange and their fully
+// unrolled networks overflow the instruction cache, so they use the compact
+// form.
 template <class E, class S>
 constexpr bool use_compact() {
     return E::kCompact && S::LOGW > S::LK;

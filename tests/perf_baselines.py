@@ -9,7 +9,7 @@ a 512 MB write, so no kernel reads a warm cache.  Times are CUDA-event
 medians per launch.  For each family the best configuration is reported:
 the reference's own sweep (bench.cu:497-521: Threads and the Sorted /
 Shared / Async switches) for V6, every thread count for CUB, every compiled
-tile for the new kernels.  Outputs are checked against numpy/the oracle.
+tile for the new kernels, in each launch form.  Outputs are checked against numpy/the oracle.
 """
 import argparse
 import ctypes
@@ -88,7 +88,10 @@ def run_case(dtype, n, arrays, dist, reps, results):
         tw = 1 << sum(base.as_tuple())
         if tw < n or tw > 4 * w:
             continue
-        for tile in (base, base.with_persistent()):
+        forms = [base, base.with_persistent()]
+        if bs.tile_info(dtype, n, 0, base).tma_form:
+            forms.append(base.with_form(2))
+        for tile in forms:
             us, res = timer.time(lambda i, o, t=tile: bs.sort_packed(dtype, i, o, n, arrays, 0, t, st), reps,
                                  False)
             record("b200sort", repr(tile), us, res)
