@@ -294,6 +294,26 @@ def reference_arm(args, wl):
     return 0
 
 
+# ---- ranks ------------------------------------------------------------------------
+# One process per GPU; ranks are independent replicas (arrays are independent),
+# so the only cross-rank operations are barriers and the maximum of the
+# per-rank device times.
+
+def reduce_max(dist, world, x, device):
+    """Maximum of x over the ranks (x itself for a single rank)."""
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_value(keys_per_rank, world, ms_max):
+    """Whole-job keys/s: every rank sorted keys_per_rank keys; the job took the slowest rank's time."""
+    return keys_per_rank * world / (ms_max * 1e-3)
+
+
 # ---- GPU arm ---------------------------------------------------------------------
 
 class Ctx:
@@ -318,11 +338,7 @@ class Ctx:
             self.dist.barrier()
 
     def max_over_ranks(self, x):
-        if self.world == 1:
-            return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.dev)
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(self.dist, self.world, x, self.dev)
 
     def sync(self):
         self.torch.cuda.synchronize(self.dev)
@@ -460,7 +476,7 @@ def run_gpu(args, wl):
             "launches_per_step": plain_launches,
             "persistent_graph_speedup": ms_plain / ms_step}}
 
-    value = total_keys * ctx.world / (ms_step * 1e-3)
+    value = weak_value(total_keys, ctx.world, ms_step)
     hbm, peak_src = peaks()
     algo_bytes = 2 * batch_bytes
     achieved = algo_bytes / (ms_step * 1e-3) / 1e9
