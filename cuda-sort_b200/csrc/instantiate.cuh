@@ -165,12 +165,12 @@ struct ClusterTile {
 };
 
 // The persistent ragged kernel of element type E.
-template <class E, int CTA, int NB, int LKA, int LKB>
+template <class E, int CTA, int NB, int LKA, int LKB, bool SB = false, int MINB = 1>
 struct Ragged {
-    static constexpr size_t SMEM = ragged_smem<E, CTA, NB, LKA, LKB>();
+    static constexpr size_t SMEM = ragged_smem<E, CTA, NB, LKA, LKB, SB>();
     static cudaError_t launch(const void* in, void* out, const int* off, const int* ids, RaggedCtl* ctl,
                               unsigned family_mask, int grid, cudaStream_t st) {
-        auto fn = k_sort_ragged<E, CTA, NB, LKA, LKB>;
+        auto fn = k_sort_ragged<E, CTA, NB, LKA, LKB, SB, MINB>;
         if (SMEM > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM));
@@ -182,7 +182,7 @@ struct Ragged {
         return cudaGetLastError();
     }
     static int resident_per_sm() {
-        auto fn = k_sort_ragged<E, CTA, NB, LKA, LKB>;
+        auto fn = k_sort_ragged<E, CTA, NB, LKA, LKB, SB, MINB>;
         if (SMEM > 48 * 1024 &&
             cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(SMEM)) != cudaSuccess)

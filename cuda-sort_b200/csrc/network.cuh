@@ -49,6 +49,15 @@ struct TeamBarrier {
         asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
     }
 };
+// The same with one shared-memory buffer per team (see single_buffer below).
+struct TeamBarrierSingle {
+    static constexpr bool kSingleBuffer = true;
+    int id;
+    int threads;
+    __device__ __forceinline__ void operator()() const {
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+    }
+};
 
 constexpr int hibit(unsigned x) {
     int b = -1;

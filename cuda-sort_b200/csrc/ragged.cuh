@@ -145,7 +145,7 @@ struct FamilyShape {
     using type = Shape<LK, LG, LW>;
 };
 
-template <class E, class S, int CTA>
+template <class E, class S, int CTA, bool SB>
 __device__ __forceinline__ void ragged_task(const typename E::Mem* in, typename E::Mem* out,
                                             const int* __restrict__ off, const int* __restrict__ ids,
                                             int first_id, int count, int local_task,
@@ -163,13 +163,14 @@ __device__ __forceinline__ void ragged_task(const typename E::Mem* in, typename 
         start = off[a];
         na = off[a + 1] - off[a];
     }
-    R* cur = reinterpret_cast<R*>(smem_raw) + size_t(team) * 2 * S::W;
-    R* nxt = cur + S::W;
+    R* cur = reinterpret_cast<R*>(smem_raw) + size_t(team) * (SB ? 1 : 2) * S::W;
+    R* nxt = SB ? cur : cur + S::W;
     R v[S::K];
     load_tile<E, S::K>(v, in + start, t * S::K, na);
     if constexpr (S::LW > 0) {
         static_assert(CTA / S::TPA <= 15, "named barrier ids");
-        network<E, S>(v, t, cur, nxt, TeamBarrier{1 + team, S::TPA});
+        if constexpr (SB) network<E, S>(v, t, cur, nxt, TeamBarrierSingle{1 + team, S::TPA});
+        else network<E, S>(v, t, cur, nxt, TeamBarrier{1 + team, S::TPA});
     } else {
         network<E, S>(v, t, cur, nxt);
     }
@@ -177,9 +178,11 @@ __device__ __forceinline__ void ragged_task(const typename E::Mem* in, typename 
 }
 
 // NB buckets (W = 8 .. 8 << (NB-1)); bucket b uses family B (K = 2^LKB)
-// when bit b of family_mask is set, else family A (K = 2^LKA).
-template <class E, int CTA, int NB, int LKA, int LKB>
-__global__ void __launch_bounds__(CTA, 1) k_sort_ragged(const typename E::Mem* in, typename E::Mem* out,
+// when bit b of family_mask is set, else family A (K = 2^LKA).  SB: one
+// shared-memory buffer per team (two barriers per shared-memory layer, half
+// the shared memory); MINB: CTAs per SM the register budget is sized for.
+template <class E, int CTA, int NB, int LKA, int LKB, bool SB, int MINB>
+__global__ void __launch_bounds__(CTA, MINB) k_sort_ragged(const typename E::Mem* in, typename E::Mem* out,
                                                         const int* __restrict__ off,
                                                         const int* __restrict__ ids, RaggedCtl* ctl,
                                                         unsigned family_mask) {
@@ -220,19 +223,19 @@ __global__ void __launch_bounds__(CTA, 1) k_sort_ragged(const typename E::Mem* i
             constexpr int L = B + kRaggedLmin;
             if (b == B) {
                 if (fam_b)
-                    ragged_task<E, typename FamilyShape<LKB, L, CTA>::type, CTA>(in, out, off, ids, s_base[B],
-                                                                                  s_count[B], local, smem_raw);
+                    ragged_task<E, typename FamilyShape<LKB, L, CTA>::type, CTA, SB>(in, out, off, ids, s_base[B],
+                                                                                      s_count[B], local, smem_raw);
                 else
-                    ragged_task<E, typename FamilyShape<LKA, L, CTA>::type, CTA>(in, out, off, ids, s_base[B],
-                                                                                  s_count[B], local, smem_raw);
+                    ragged_task<E, typename FamilyShape<LKA, L, CTA>::type, CTA, SB>(in, out, off, ids, s_base[B],
+                                                                                      s_count[B], local, smem_raw);
             }
         });
     }
 }
 
-// Shared memory of k_sort_ragged: the largest per-CTA double buffer over the
-// buckets that use it.
-template <class E, int CTA, int NB, int LKA, int LKB>
+// Shared memory of k_sort_ragged: the largest per-CTA buffer (double, or
+// single when SB) over the buckets that use it.
+template <class E, int CTA, int NB, int LKA, int LKB, bool SB>
 constexpr size_t ragged_smem() {
     size_t best = 0;
     for (int b = 0; b < NB; ++b) {
@@ -242,7 +245,7 @@ constexpr size_t ragged_smem() {
             const int rest = L - k;
             const int lw = rest > 5 ? rest - 5 : 0;
             if (lw > 0) {
-                const size_t bytes = 2 * size_t(CTA) * (size_t(1) << k) * sizeof(typename E::Reg);
+                const size_t bytes = (SB ? 1 : 2) * size_t(CTA) * (size_t(1) << k) * sizeof(typename E::Reg);
                 if (bytes > best) best = bytes;
             }
         }
