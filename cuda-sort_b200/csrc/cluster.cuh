@@ -24,11 +24,6 @@ namespace b200s {
 
 namespace cg = cooperative_groups;
 
-struct CtaBarrierSingle {
-    static constexpr bool kSingleBuffer = true;
-    __device__ __forceinline__ void operator()() const { __syncthreads(); }
-};
-
 template <class E, class S, int LC, unsigned MASK, bool SB>
 __device__ __forceinline__ void cluster_layer(typename E::Reg (&v)[S::K], const int t, const int rank,
                                               typename E::Reg*& cur, typename E::Reg*& nxt) {

@@ -11,11 +11,12 @@
 
 namespace b200s {
 
-template <class E, int LK, int LG, int LW>
+// SB: single-buffered shared-memory layers (multi-warp tiles only).
+template <class E, int LK, int LG, int LW, bool SB = false>
 struct Packed {
     using S = Shape<LK, LG, LW>;
     static constexpr int CTA = LW > 0 ? S::TPA : (S::TPA >= 128 ? S::TPA : 128);
-    static constexpr size_t SMEM = LW > 0 ? 2 * size_t(S::W) * sizeof(typename E::Reg) : 0;
+    static constexpr size_t SMEM = LW > 0 ? (SB ? 1 : 2) * size_t(S::W) * sizeof(typename E::Reg) : 0;
 
     // The opt-in above 48 KB is per kernel and per device; WHICH keeps one
     // record per kernel of this tile (0 packed, 1 list, 2 persistent).
@@ -34,7 +35,7 @@ struct Packed {
     }
     static cudaError_t launch(const void* in, void* out, int n, long long arrays, long long grid,
                               cudaStream_t st) {
-        auto fn = k_sort_packed<E, S, CTA>;
+        auto fn = k_sort_packed<E, S, CTA, SB>;
         cudaError_t e = prepare<0>(reinterpret_cast<const void*>(fn));
         if (e != cudaSuccess) return e;
         fn<<<dim3(unsigned(grid)), dim3(CTA), SMEM, st>>>(
@@ -43,7 +44,7 @@ struct Packed {
     }
     static cudaError_t launch_list(const void* in, void* out, const int* off, const int* ids, int count,
                                    cudaStream_t st) {
-        auto fn = k_sort_idlist<E, S, CTA>;
+        auto fn = k_sort_idlist<E, S, CTA, SB>;  // the same buffering as SMEM
         cudaError_t e = prepare<1>(reinterpret_cast<const void*>(fn));
         if (e != cudaSuccess) return e;
         const int grid = (count + CTA / S::TPA - 1) / (CTA / S::TPA);
@@ -55,7 +56,7 @@ struct Packed {
     // more than the batch needs.
     static cudaError_t launch_pf(const void* in, void* out, int n, long long arrays, long long grid,
                                  cudaStream_t st) {
-        auto fn = k_sort_packed_pf<E, S, CTA>;
+        auto fn = k_sort_packed_pf<E, S, CTA, SB>;
         cudaError_t e = prepare<2>(reinterpret_cast<const void*>(fn));
         if (e != cudaSuccess) return e;
         static std::atomic<int> resident[64];
@@ -79,7 +80,7 @@ struct Packed {
         return cudaGetLastError();
     }
     static cudaError_t attrs(cudaFuncAttributes* a) {
-        return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(k_sort_packed<E, S, CTA>));
+        return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(k_sort_packed<E, S, CTA, SB>));
     }
     static KernelEntry entry(int dtype) {
         return KernelEntry{dtype,   E::kStable ? 1 : 0, LK,     LG,         LW,

@@ -42,6 +42,11 @@ __device__ __forceinline__ void sfor(F&& f) {
 struct CtaBarrier {
     __device__ __forceinline__ void operator()() const { __syncthreads(); }
 };
+// __syncthreads with one shared-memory buffer (see single_buffer below).
+struct CtaBarrierSingle {
+    static constexpr bool kSingleBuffer = true;
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
 struct TeamBarrier {
     int id;
     int threads;
@@ -336,7 +341,9 @@ __device__ __forceinline__ void store_tile(const typename E::Reg (&v)[K], typena
 // a CTA holds CTA/TPA groups and strides over the batch.  The loop bound is
 // uniform across the CTA, so groups past the end sort padding and store
 // nothing, and every warp-wide shuffle and barrier sees all its threads.
-template <class E, class S, int CTA>
+// SB: one shared-memory buffer (two barriers per shared-memory layer, half the
+// shared memory, more CTAs per SM) instead of two.
+template <class E, class S, int CTA, bool SB = false>
 __global__ void __launch_bounds__(CTA) k_sort_packed(const typename E::Mem* in,
                                                      typename E::Mem* out, int n,
                                                      long long arrays) {
@@ -346,7 +353,7 @@ __global__ void __launch_bounds__(CTA) k_sort_packed(const typename E::Mem* in,
     constexpr int APC = CTA / S::TPA;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* cur = reinterpret_cast<R*>(smem_raw);
-    R* nxt = cur + S::W;
+    R* nxt = SB ? cur : cur + S::W;
     const int slot = int(threadIdx.x) / S::TPA;
     const int t = int(threadIdx.x) % S::TPA;
     for (long long first = (long long)blockIdx.x * APC; first < arrays;
@@ -356,7 +363,8 @@ __global__ void __launch_bounds__(CTA) k_sort_packed(const typename E::Mem* in,
         const long long off = (a < arrays ? a : 0) * (long long)n;
         R v[S::K];
         load_tile<E, S::K>(v, in + off, t * S::K, na);
-        network<E, S>(v, t, cur, nxt);
+        if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{});
+        else network<E, S>(v, t, cur, nxt);
         store_tile<E, S::K>(v, out + off, t * S::K, na);
     }
 }
@@ -365,7 +373,7 @@ __global__ void __launch_bounds__(CTA) k_sort_packed(const typename E::Mem* in,
 // walks the batch with a stride of the whole grid, loading the next array's
 // tile into registers before sorting the current one, so that the global
 // loads of one array overlap the comparator layers of the previous one.
-template <class E, class S, int CTA>
+template <class E, class S, int CTA, bool SB = false>
 __global__ void __launch_bounds__(CTA) k_sort_packed_pf(const typename E::Mem* in,
                                                         typename E::Mem* out, int n,
                                                         long long arrays) {
@@ -373,7 +381,7 @@ __global__ void __launch_bounds__(CTA) k_sort_packed_pf(const typename E::Mem* i
     constexpr int APC = CTA / S::TPA;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* cur = reinterpret_cast<R*>(smem_raw);
-    R* nxt = cur + S::W;
+    R* nxt = SB ? cur : cur + S::W;
     const int slot = int(threadIdx.x) / S::TPA;
     const int t = int(threadIdx.x) % S::TPA;
     const long long stride = (long long)gridDim.x * APC;
@@ -389,7 +397,8 @@ __global__ void __launch_bounds__(CTA) k_sort_packed_pf(const typename E::Mem* i
         const long long an = a + stride;
         R w[S::K];
         load_tile<E, S::K>(w, in + (an < arrays ? an : 0) * (long long)n, t * S::K, an < arrays ? n : 0);
-        network<E, S>(v, t, cur, nxt);
+        if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{});
+        else network<E, S>(v, t, cur, nxt);
         if (a < arrays) store_tile<E, S::K>(v, out + a * (long long)n, t * S::K, n);
 #pragma unroll
         for (int q = 0; q < S::K; ++q) v[q] = w[q];

@@ -255,7 +255,7 @@ constexpr size_t ragged_smem() {
 
 // Plain per-length launches: every array of the id list has the same length
 // class; one group per array, grid covers the list.
-template <class E, class S, int CTA>
+template <class E, class S, int CTA, bool SB = false>
 __global__ void __launch_bounds__(CTA) k_sort_idlist(const typename E::Mem* in, typename E::Mem* out,
                                                      const int* __restrict__ off, const int* __restrict__ ids,
                                                      int count) {
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(CTA) k_sort_idlist(const typename E::Mem* in, 
     constexpr int APC = CTA / S::TPA;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* cur = reinterpret_cast<R*>(smem_raw);
-    R* nxt = cur + S::W;
+    R* nxt = SB ? cur : cur + S::W;  // the launch passes 1 or 2 buffers of W elements
     const int slot = int(threadIdx.x) / S::TPA;
     const int t = int(threadIdx.x) % S::TPA;
     for (long long first = (long long)blockIdx.x * APC; first < count; first += (long long)gridDim.x * APC) {
@@ -277,7 +277,8 @@ __global__ void __launch_bounds__(CTA) k_sort_idlist(const typename E::Mem* in, 
         }
         R v[S::K];
         load_tile<E, S::K>(v, in + start, t * S::K, na);
-        network<E, S>(v, t, cur, nxt);
+        if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{});
+        else network<E, S>(v, t, cur, nxt);
         store_tile<E, S::K>(v, out + start, t * S::K, na);
     }
 }

@@ -13,10 +13,12 @@ static void add_rec(std::vector<KernelEntry>& o) {
     o.push_back(Packed<E, 4, 3, 0>::entry(D));
     o.push_back(Packed<E, 4, 4, 0>::entry(D));
     o.push_back(Packed<E, 4, 5, 0>::entry(D));  // W = 512
-    o.push_back(Packed<E, 4, 5, 1>::entry(D));  // W = 1024
-    o.push_back(Packed<E, 4, 5, 2>::entry(D));
-    o.push_back(Packed<E, 4, 5, 3>::entry(D));
-    o.push_back(Packed<E, 4, 5, 4>::entry(D));  // W = 8192, 512 threads
+    // Multi-warp tiles single-buffer their shared-memory layers: more CTAs
+    // per SM (the record kernels are ALU bound, residency hides latency).
+    o.push_back(Packed<E, 4, 5, 1, true>::entry(D));  // W = 1024
+    o.push_back(Packed<E, 4, 5, 2, true>::entry(D));
+    o.push_back(Packed<E, 4, 5, 3, true>::entry(D));
+    o.push_back(Packed<E, 4, 5, 4, true>::entry(D));  // W = 8192, 512 threads
 }
 
 void register_rec(std::vector<KernelEntry>& o) {
