@@ -425,6 +425,12 @@ b200s_status b200s_tma_timeouts(int64_t* count) {
     return B200S_OK;
 }
 
+b200s_status b200s_test_stall_tma_loads(int32_t enable) {
+    if (!tma_set_extra_tx(enable ? 16u : 0u))
+        return set_error(B200S_ERR_CUDA, "writing the TMA status word failed");
+    return B200S_OK;
+}
+
 b200s_status b200s_load_tile_table(const char* path, int32_t* applied) {
     if (!path) return set_error(B200S_ERR_INVALID_ARGUMENT, "b200s_load_tile_table: null path");
     TableRows rows;

@@ -70,6 +70,7 @@ struct TmaEntry {
 };
 const std::vector<TmaEntry>& tma_registry();
 int64_t tma_timeouts();  // CTAs of the TMA kernels that gave up waiting for a load
+bool tma_set_extra_tx(unsigned int bytes);  // failure-detection test hook
 
 void register_ragged_i32(std::vector<RaggedEntry>& out);
 void register_ragged_rec(std::vector<RaggedEntry>& out);

@@ -179,6 +179,11 @@ const std::vector<TmaEntry>& tma_registry() {
     return all;
 }
 
+bool tma_set_extra_tx(unsigned int bytes) {
+    TmaStatus* p = status_ptr();
+    return p && cudaMemcpy(&p->extra_tx, &bytes, sizeof(bytes), cudaMemcpyHostToDevice) == cudaSuccess;
+}
+
 int64_t tma_timeouts() {
     TmaStatus s{};
     if (cudaMemcpyFromSymbol(&s, g_tma_status, sizeof(s)) != cudaSuccess) return -1;

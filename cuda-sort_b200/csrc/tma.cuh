@@ -90,8 +90,13 @@ constexpr long long kWaitLimit = 2000000000LL;
 }  // namespace tma
 
 // Counts CTAs that gave up waiting for a TMA load (0 in a healthy run).
+// extra_tx is a test hook: bytes added to every load's expected transaction
+// count, so that no chunk ever completes and the bounded wait runs out
+// (0 outside the failure-detection test).
 struct TmaStatus {
     unsigned long long timeouts;
+    unsigned int extra_tx;
+    unsigned int reserved;
 };
 
 template <class E, class S, int CTA, int DEPTH>
@@ -115,7 +120,7 @@ __global__ void __launch_bounds__(CTA) k_sort_packed_tma(const __grid_constant__
     const int slot = tid / S::TPA;
     const int t = tid % S::TPA;
     const uint32_t buf_bytes = (uint32_t(APC * rows * 128) + 1023u) & ~1023u;
-    const uint32_t box_bytes = uint32_t(APC * rows * 128);
+    const uint32_t box_bytes = uint32_t(APC * rows * 128) + status->extra_tx;
     const long long chunks = (arrays + APC - 1) / APC;
     const int valid_chunks = (n * EB) / 16;  // 16-byte chunks of one array
     // 1024-byte aligned base for the swizzle pattern

@@ -125,6 +125,12 @@ b200s_status b200s_tile_info_get(b200s_dtype dtype, uint32_t flags, const b200s_
  * waiting for a load after about a second (each left its chunk unsorted).
  * Always 0 unless the device misbehaves; a cumulative count. */
 b200s_status b200s_tma_timeouts(int64_t* count);
+/* Test hook for failure detection: while enabled, every TMA-pipelined launch
+ * on the current device expects 16 bytes more per chunk than its loads
+ * deliver, so its bounded wait runs out (about a second per CTA), each CTA
+ * counts itself in b200s_tma_timeouts and returns with its chunks unsorted;
+ * nothing faults.  Disable before any real work. */
+b200s_status b200s_test_stall_tma_loads(int32_t enable);
 /* Replace rows of the default tile table from a CSV file; '#' starts a
  * comment.  Packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps
  * [,form] (form: 0, 1 or 2 as b200s_tile.persistent).  Ragged rows: r,dtype,flags,log2_w,family (0: the larger

@@ -43,6 +43,7 @@ def timeouts():
 
 @pytest.mark.parametrize("dtype,lk,lg", TMA_TILES)
 def test_tma_form_matches_oracle(dtype, lk, lg):
+    t0 = timeouts()
     eb = bs.ELEM_BYTES[dtype]
     w = 1 << (lk + lg)
     row = 128 // eb                       # elements per 128-byte row
@@ -61,10 +62,11 @@ def test_tma_form_matches_oracle(dtype, lk, lg):
                     got = sort_with(dtype, tile, data, n, arrays, inplace)
                     assert np.array_equal(got, want), "tile K=%d G=%d n=%d arrays=%d %s inplace=%s" % (
                         1 << lk, tpa, n, arrays, dist, inplace)
-    assert timeouts() == 0
+    assert timeouts() == t0
 
 
 def test_tma_form_large_batches_every_distribution():
+    t0 = timeouts()
     for dtype, n, arrays in ((bs.I32, 1024, 4096), (bs.I32_I32, 32, 131072), (bs.I32_I32, 256, 16384)):
         t = bs.default_tile(dtype, n)
         tile = bs.Tile(t.log2_items, t.log2_lanes, t.log2_warps, 0, 2, 0)
@@ -72,7 +74,7 @@ def test_tma_form_large_batches_every_distribution():
             data = workloads.make_packed(dtype, n, arrays, dist, seed=11, extremes=True)
             got = sort_with(dtype, tile, data, n, arrays, False)
             assert np.array_equal(got, expected(dtype, data, n, arrays)), (dtype, n, dist)
-    assert timeouts() == 0
+    assert timeouts() == t0
 
 
 def test_tma_form_falls_back_when_rows_do_not_align():
@@ -94,8 +96,35 @@ def test_tma_form_falls_back_when_rows_do_not_align():
 def test_tma_form_alternating_lengths_of_one_tile():
     # one kernel serves every length its tile covers; shared-memory needs differ
     # by length, so launches alternate long, short, long
+    t0 = timeouts()
     dtype, tile = bs.I32_I32, bs.Tile(4, 5, 0, 0, 2, 0)     # W = 512 records
     for n in (512, 16, 512, 256, 512):
         data = workloads.make_packed(dtype, n, 700, "distinct16", seed=n, extremes=True)
         assert np.array_equal(sort_with(dtype, tile, data, n, 700, False), expected(dtype, data, n, 700)), n
-    assert timeouts() == 0
+    assert timeouts() == t0
+
+
+def test_tma_wait_runs_out_without_a_fault():
+    """Failure detection: a load that never completes (the expected byte count
+    is raised above what the copy delivers) ends the bounded wait; the CTA
+    counts itself, returns, and the context stays usable."""
+    import torch
+    stall = bs.declare("b200s_test_stall_tma_loads", ctypes.c_int, [ctypes.c_int32])
+    dtype, n, arrays = bs.I32_I32, 256, 8            # one chunk: one CTA
+    tile = bs.Tile(4, 4, 0, 0, 2, 0)
+    data = workloads.make_packed(dtype, n, arrays, "uniform", seed=5)
+    before = timeouts()
+    d_in = to_device(data)
+    d_out = empty_device(d_in.numel())
+    d_out.fill_(0)
+    torch.cuda.synchronize()
+    assert stall(1) == 0
+    try:
+        bs.sort_packed(dtype, d_in.data_ptr(), d_out.data_ptr(), n, arrays, 0, tile, stream_handle())
+        torch.cuda.synchronize()
+    finally:
+        assert stall(0) == 0
+    assert timeouts() == before + 1
+    assert not from_device(d_out[:data.nbytes], bs.NP_DTYPES[dtype])["key"].any()   # chunk left unwritten
+    # the device keeps working
+    assert np.array_equal(sort_with(dtype, tile, data, n, arrays, False), expected(dtype, data, n, arrays))
