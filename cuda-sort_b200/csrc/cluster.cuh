@@ -127,8 +127,10 @@ __device__ __forceinline__ void cluster_network(typename E::Reg (&v)[S::K], cons
 // One cluster per array, clusters striding over the batch.  Packed batches
 // (ids == nullptr): array a at a*n, count = arrays.  Id lists: array ids[i]
 // of a CSR batch, count read from *d_count (or `arrays` when d_count is null).
-template <class E, class S, int LC, bool SB>
-__global__ void __launch_bounds__(S::TPA, 1) k_sort_cluster(const typename E::Mem* in, typename E::Mem* out,
+// MINB: CTAs per SM the register budget is sized for (2 with single-buffered
+// shared memory lets two clusters' CTAs share an SM).
+template <class E, class S, int LC, bool SB, int MINB = 1>
+__global__ void __launch_bounds__(S::TPA, MINB) k_sort_cluster(const typename E::Mem* in, typename E::Mem* out,
                                                             int n, long long arrays, const int* off,
                                                             const int* ids, const int* d_count) {
     using R = typename E::Reg;

@@ -90,7 +90,7 @@ struct Packed {
 };
 
 // A cluster of 2^LC CTAs per array (SB: single-buffered shared memory).
-template <class E, int LK, int LG, int LW, int LC, bool SB>
+template <class E, int LK, int LG, int LW, int LC, bool SB, int MINB = 1>
 struct ClusterTile {
     using S = Shape<LK, LG, LW>;
     static constexpr int CTA = S::TPA;
@@ -119,7 +119,7 @@ struct ClusterTile {
         if (e != cudaSuccess) return e;
         int v = cache[dev & 63].load(std::memory_order_relaxed);
         if (v == 0) {
-            auto fn = k_sort_cluster<E, S, LC, SB>;
+            auto fn = k_sort_cluster<E, S, LC, SB, MINB>;
             e = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      int(SMEM));
             if (e != cudaSuccess) return e;
@@ -142,7 +142,7 @@ struct ClusterTile {
         if (clusters < 1) clusters = 1;
         cudaLaunchAttribute attr;
         cudaLaunchConfig_t cfg = config(clusters, st, &attr);
-        return cudaLaunchKernelEx(&cfg, k_sort_cluster<E, S, LC, SB>, static_cast<const typename E::Mem*>(in),
+        return cudaLaunchKernelEx(&cfg, k_sort_cluster<E, S, LC, SB, MINB>, static_cast<const typename E::Mem*>(in),
                                   static_cast<typename E::Mem*>(out), n, arrays, off, ids, d_count);
     }
     static cudaError_t launch(const void* in, void* out, int n, long long arrays, long long, cudaStream_t st) {
@@ -157,7 +157,7 @@ struct ClusterTile {
         return run(in, out, 0, max_count, off, ids, d_count, max_count, st);
     }
     static cudaError_t attrs(cudaFuncAttributes* a) {
-        return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(k_sort_cluster<E, S, LC, SB>));
+        return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(k_sort_cluster<E, S, LC, SB, MINB>));
     }
     static KernelEntry entry(int dtype) {
         return KernelEntry{dtype, E::kStable ? 1 : 0, LK, LG, LW, CTA, S::LOGW + LC, SMEM, 1, &launch, &attrs,

@@ -199,9 +199,11 @@ typedef struct b200s_session b200s_session;
 b200s_status b200s_session_create(b200s_session** out, int32_t device);
 b200s_status b200s_session_destroy(b200s_session* session);
 /* Same as b200s_sort_packed, on host buffers: the batch is copied to the
- * device in chunks, sorted and copied back, with the copies of one chunk
- * overlapping the sort of another.  Pinned host buffers give full PCIe
- * bandwidth.  Returns after the output is in h_out. */
+ * device in chunks of whole arrays (a quarter of the batch, 2 to 64 MB), each
+ * chunk sorted after its copy on one stream and copied back on another, so
+ * that the copy back of one chunk overlaps the copy in of the next.  Pinned
+ * host buffers give full PCIe bandwidth.  Returns after the output is in
+ * h_out. */
 b200s_status b200s_sort_packed_host(b200s_session* session, b200s_dtype dtype, const void* h_in,
                                     void* h_out, int32_t n, int64_t arrays, uint32_t flags);
 

@@ -182,3 +182,22 @@ def test_host_session_matches_device_path():
                 h_out = np.empty_like(data)
                 s.sort_host(dtype, data.ctypes.data, h_out.ctypes.data, n, arrays)
                 assert np.array_equal(h_out, got)
+
+
+def test_host_session_ring_wraps_over_many_chunks():
+    """A 327 MB batch is cut into 64 MB chunks: more chunks than device slots,
+    so copy-ins wait for earlier copy-outs of the same slot."""
+    import torch
+    n, arrays = 4096, 20000
+    data = workloads.make_packed(bs.I32, n, arrays, "uniform", seed=20000, extremes=True)
+    pinned = torch.from_numpy(data.view(np.uint8).copy()).pin_memory()
+    out = torch.empty_like(pinned).pin_memory()
+    with bs.Session(0) as s:
+        s.sort_host(bs.I32, pinned.data_ptr(), out.data_ptr(), n, arrays)
+        got = out.numpy().view(bs.NP_DTYPES[bs.I32])
+        assert np.array_equal(got, gpu_sort(bs.I32, data, n, arrays))
+        assert np.array_equal(got.reshape(arrays, n), np.sort(data.reshape(arrays, n), axis=1))
+        # the same session again with a smaller batch (slots already large enough)
+        s.sort_host(bs.I32, pinned.data_ptr(), out.data_ptr(), n, 100)
+        assert np.array_equal(out.numpy().view(bs.NP_DTYPES[bs.I32])[:100 * n].reshape(100, n),
+                              np.sort(data[:100 * n].reshape(100, n), axis=1))
