@@ -577,6 +577,13 @@ b200s_status b200s_sort_packed_host(b200s_session* s, b200s_dtype dtype, const v
     }
     const char* src = static_cast<const char*>(h_in);
     char* dst = static_cast<char*>(h_out);
+    // On a failure part way, wait for the copies already queued so that none
+    // touches the caller's buffers after the call returns.
+    auto drain = [s](b200s_status status) {
+        cudaStreamSynchronize(s->in);
+        cudaStreamSynchronize(s->out);
+        return status;
+    };
     long long chunk = 0;
     for (long long first = 0; first < arrays; first += per_chunk, ++chunk) {
         const long long count = std::min<long long>(per_chunk, arrays - first);
@@ -584,18 +591,18 @@ b200s_status b200s_sort_packed_host(b200s_session* s, b200s_dtype dtype, const v
         const int k = int(chunk % b200s_session::kSlots);
         // the slot's previous chunk must have left before this one lands
         e = cudaStreamWaitEvent(s->in, s->freed[k], 0);
-        if (e != cudaSuccess) return cuda_error(e, "session slot wait");
+        if (e != cudaSuccess) return drain(cuda_error(e, "session slot wait"));
         e = cudaMemcpyAsync(s->dbuf[k], src + size_t(first) * array_bytes, bytes, cudaMemcpyHostToDevice, s->in);
-        if (e != cudaSuccess) return cuda_error(e, "host-to-device copy");
+        if (e != cudaSuccess) return drain(cuda_error(e, "host-to-device copy"));
         st = launch_packed(idx, persistent, s->dbuf[k], s->dbuf[k], n, count, s->in);
-        if (st != B200S_OK) return st;
+        if (st != B200S_OK) return drain(st);
         e = cudaEventRecord(s->sorted[k], s->in);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(s->out, s->sorted[k], 0);
-        if (e != cudaSuccess) return cuda_error(e, "session sort event");
+        if (e != cudaSuccess) return drain(cuda_error(e, "session sort event"));
         e = cudaMemcpyAsync(dst + size_t(first) * array_bytes, s->dbuf[k], bytes, cudaMemcpyDeviceToHost, s->out);
-        if (e != cudaSuccess) return cuda_error(e, "device-to-host copy");
+        if (e != cudaSuccess) return drain(cuda_error(e, "device-to-host copy"));
         e = cudaEventRecord(s->freed[k], s->out);
-        if (e != cudaSuccess) return cuda_error(e, "session slot event");
+        if (e != cudaSuccess) return drain(cuda_error(e, "session slot event"));
     }
     e = cudaStreamSynchronize(s->in);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->out);
