@@ -138,6 +138,53 @@ def alu_roofline(dtype, tile, elements, seconds, sm_mhz):
                                     "records: 2.5 and 5 (compare + selects)"}
 
 
+_ONCHIP = {}
+
+
+def onchip_peaks(device, cluster=0):
+    """Shared-memory (and, for cluster > 1, distributed-shared-memory) bandwidth
+    of this device in GB/s, measured once per process by the probes of
+    cuda-sort_b200/harness/onchip_peak.cu."""
+    key = (device, cluster)
+    if key not in _ONCHIP:
+        lib = ctypes.CDLL(os.path.join(ROOT, "cuda-sort_b200", "libb200sort_onchip.so"))
+        rd, cp = ctypes.c_double(0), ctypes.c_double(0)
+        out = {}
+        if lib.onchip_smem_gbs(device, ctypes.byref(rd), ctypes.byref(cp)) == 0:
+            out.update(smem_read_gbs=rd.value, smem_copy_gbs=cp.value)
+        if cluster > 1:
+            ds = ctypes.c_double(0)
+            if lib.onchip_dsmem_gbs(device, cluster, ctypes.byref(ds)) == 0:
+                out["dsmem_read_gbs"] = ds.value
+        _ONCHIP[key] = out
+    return _ONCHIP[key]
+
+
+def onchip_roofline(widths, elem_bytes, seconds, t_hbm, device, lc=0, arrays=0):
+    """On-chip bound: every bitonic stage whose span leaves a 1024-element
+    window costs at least one write and one read of the tile, so
+    bytes = sum 2 * W * elem_bytes * max(0, log2 W - 10) over the arrays,
+    against the measured shared-memory copy rate; fraction = the larger of the
+    HBM and on-chip times over the measured time.  For cluster kernels also the
+    distributed-shared-memory reads: every cross-CTA layer reads the whole tile
+    from peers once."""
+    widths = np.asarray(widths, dtype=np.int64)
+    logw = np.log2(widths).astype(np.int64)
+    r = np.maximum(0, logw - 10)
+    nbytes = float(np.sum(2 * widths * elem_bytes * r))
+    pk = onchip_peaks(device, 1 << lc if lc else 0)
+    out = {"bytes": nbytes, "model": "sum 2*W*elem_bytes*max(0, log2 W - 10) at the measured shared-memory copy rate"}
+    if "smem_copy_gbs" in pk:
+        t_on = nbytes / (pk["smem_copy_gbs"] * 1e9)
+        out.update(pk, t_us=t_on * 1e6, frac=t_on / seconds, frac_max_hbm_onchip=max(t_hbm, t_on) / seconds)
+    if lc and "dsmem_read_gbs" in pk:
+        layers = lc * (lc + 1) // 2
+        dbytes = float(arrays) * layers * float(widths.max()) * elem_bytes
+        t_ds = dbytes / (pk["dsmem_read_gbs"] * 1e9)
+        out["dsmem"] = {"bytes": dbytes, "cross_cta_layers": layers, "t_us": t_ds * 1e6, "frac": t_ds / seconds}
+    return out
+
+
 def traffic_for(workload):
     """DRAM bytes per launch of the sort kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "traffic.txt")
@@ -483,9 +530,18 @@ def run_gpu(args, wl):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "peak_source": peak_src, "traffic": traffic_for(args.workload),
                 "algorithmic_bytes_per_launch": algo_bytes, "kernel": kernel, "launch_us": ms_step * 1e3}
+    t_hbm = algo_bytes / (hbm * 1e9)
     if wl["kind"] == "packed":
         w = 1 << (eff.log2_items + eff.log2_lanes + eff.log2_warps + eff.log2_ctas)
         roofline["alu"] = alu_roofline(dtype, eff, wl["arrays"] * w, ms_step * 1e-3, clocks.get("sm_mhz"))
+        wmin = 1 << max(5, int(wl["n"] - 1).bit_length())
+        roofline["onchip"] = onchip_roofline(np.full(wl["arrays"], wmin), bs.ELEM_BYTES[dtype], ms_step * 1e-3,
+                                             t_hbm, ctx.local, lc=eff.log2_ctas, arrays=wl["arrays"])
+    else:
+        lens = np.diff(off).astype(np.int64)
+        lens = lens[lens > 0]
+        widths = np.left_shift(1, np.maximum(5, np.ceil(np.log2(np.maximum(lens, 1))).astype(np.int64)))
+        roofline["onchip"] = onchip_roofline(widths, bs.ELEM_BYTES[dtype], ms_step * 1e-3, t_hbm, ctx.local)
 
     e2e = None
     if not args.no_e2e:

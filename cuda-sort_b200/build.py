@@ -19,6 +19,7 @@ CUB_LIB = os.path.join(HERE, "libb200sort_cub.so")
 HARNESS = os.path.join(HERE, "harness")
 LOADGEN_LIB = os.path.join(HERE, "libb200sort_loadgen.so")
 BENCH_CLI = os.path.join(HERE, "b200sort_bench")
+ONCHIP_LIB = os.path.join(HERE, "libb200sort_onchip.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -80,6 +81,7 @@ def build(verbose=False, extra=None, jobs=None):
     build_cub_baseline()
     build_loadgen()
     build_bench_cli()
+    build_onchip()
     if verbose:
         print("built", LIB, CUB_LIB, LOADGEN_LIB, BENCH_CLI)
     return LIB
@@ -109,6 +111,18 @@ def build_loadgen():
     if r.returncode != 0:
         raise RuntimeError("load generator build failed:\n" + r.stdout + r.stderr)
     return LOADGEN_LIB
+
+
+def build_onchip():
+    """Shared-memory and distributed-shared-memory bandwidth probes (the on-chip roofline's peaks)."""
+    src = os.path.join(HARNESS, "onchip_peak.cu")
+    if os.path.exists(ONCHIP_LIB) and os.path.getmtime(ONCHIP_LIB) >= os.path.getmtime(src):
+        return ONCHIP_LIB
+    cmd = [NVCC] + ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", src, "-o", ONCHIP_LIB]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("on-chip probe build failed:\n" + r.stdout + r.stderr)
+    return ONCHIP_LIB
 
 
 def build_bench_cli():

@@ -162,12 +162,12 @@ void register_tma(std::vector<TmaEntry>& o) {
     o.push_back(PackedTma<ElemI32, 5, 2, 128>::entry(0));  // W = 128
     o.push_back(PackedTma<ElemI32, 5, 0, 128>::entry(0));  // W = 32
     // IntAndData records (reference tie order)
-    o.push_back(PackedTma<ElemRecI32, 4, 1, 128>::entry(1));  // W = 32
-    o.push_back(PackedTma<ElemRecI32, 4, 2, 128>::entry(1));  // W = 64
-    o.push_back(PackedTma<ElemRecI32, 4, 3, 128>::entry(1));  // W = 128
-    o.push_back(PackedTma<ElemRecI32, 4, 4, 128>::entry(1));  // W = 256
-    o.push_back(PackedTma<ElemRecI32, 4, 5, 128>::entry(1));  // W = 512
-    o.push_back(PackedTma<ElemRecI32, 5, 5, 128>::entry(1));  // W = 1024
+    o.push_back(PackedTma<ElemRecI32, 4, 1, 64>::entry(1));  // W = 32
+    o.push_back(PackedTma<ElemRecI32, 4, 2, 64>::entry(1));  // W = 64
+    o.push_back(PackedTma<ElemRecI32, 4, 3, 64>::entry(1));  // W = 128
+    o.push_back(PackedTma<ElemRecI32, 4, 4, 64>::entry(1));  // W = 256
+    o.push_back(PackedTma<ElemRecI32, 4, 5, 64>::entry(1));  // W = 512
+    o.push_back(PackedTma<ElemRecI32, 5, 5, 64>::entry(1));  // W = 1024
 }
 
 const std::vector<TmaEntry>& tma_registry() {
