@@ -57,7 +57,16 @@ __device__ __forceinline__ void cluster_layer(typename E::Reg (&v)[S::K], const 
 // Cross-CTA layer with a run-time CTA mask cm: the partner of (rank, t, q)
 // is (rank ^ cm, t ^ TM, q ^ RM); a reflection flips every lower bit (RM, TM
 // all ones), a merge only the CTA bit.
-template <class E, class S, unsigned RM, unsigned TM>
+// Cluster barrier for warps that reach it from different code (no .aligned):
+// arrive with release, wait with acquire semantics at cluster scope.
+__device__ __forceinline__ void cluster_sync_unaligned() {
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+
+// LIVE == false: the copy run by a warp that holds only padding; it
+// publishes and meets both cluster barriers but reads nothing.  UA: warps of
+// the cluster run different copies (unaligned barriers).
+template <class E, class S, unsigned RM, unsigned TM, bool LIVE, bool UA>
 __device__ __forceinline__ void cta_layer_rt(typename E::Reg (&v)[S::K], const int t, const int rank, const int cm,
                                              const bool upper, typename E::Reg* cur) {
     using R = typename E::Reg;
@@ -66,51 +75,66 @@ __device__ __forceinline__ void cta_layer_rt(typename E::Reg (&v)[S::K], const i
         constexpr int q = decltype(qc)::value;
         cur[q * S::TPA + t] = v[q];
     });
-    cluster.sync();
-    const R* remote = cluster.map_shared_rank(cur, rank ^ cm);
-    sfor<0, S::K>([&](auto qc) {
-        constexpr int q = decltype(qc)::value;
-        const R b = remote[(q ^ int(RM)) * S::TPA + (t ^ int(TM))];
-        v[q] = E::pick(v[q], b, upper);
-    });
-    cluster.sync();
+    if constexpr (UA) cluster_sync_unaligned();
+    else cluster.sync();
+    if constexpr (LIVE) {
+        const R* remote = cluster.map_shared_rank(cur, rank ^ cm);
+        sfor<0, S::K>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            const R b = remote[(q ^ int(RM)) * S::TPA + (t ^ int(TM))];
+            v[q] = E::pick(v[q], b, upper);
+        });
+    }
+    if constexpr (UA) cluster_sync_unaligned();
+    else cluster.sync();
 }
 
 // The cluster network with the stages above one CTA as a run-time loop
 // (one copy of their code), for elements whose unrolled network would not
-// fit the instruction cache.
-template <class E, class S, int LC, bool SB>
+// fit the instruction cache.  LIVE == false: the copy for a warp that holds
+// only padding (see network_compact): it publishes and synchronises only,
+// through the same barriers in the same order.
+template <class E, class S, int LC, bool SB, bool LIVE, bool UA>
 __device__ __forceinline__ void cluster_network_compact(typename E::Reg (&v)[S::K], const int t, const int rank,
                                                         typename E::Reg*& cur, typename E::Reg*& nxt) {
     constexpr int LOCAL = S::LOGW;
     // stages inside one CTA
-    if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{});
-    else network<E, S>(v, t, cur, nxt, CtaBarrier{});
+    if constexpr (SB) network_compact<E, S, LIVE, UA>(v, t, cur, nxt, CtaBarrierSingle{});
+    else network_compact<E, S, LIVE, UA>(v, t, cur, nxt, CtaBarrier{});
 #pragma unroll 1
     for (int st = LOCAL; st < LOCAL + LC; ++st) {
-        cta_layer_rt<E, S, unsigned(S::K - 1), unsigned(S::TPA - 1)>(v, t, rank, (2 << (st - LOCAL)) - 1,
-                                                                        (rank >> (st - LOCAL)) & 1, cur);
+        cta_layer_rt<E, S, unsigned(S::K - 1), unsigned(S::TPA - 1), LIVE, UA>(
+            v, t, rank, (2 << (st - LOCAL)) - 1, (rank >> (st - LOCAL)) & 1, cur);
 #pragma unroll 1
         for (int j = st - 1; j >= LOCAL; --j)
-            cta_layer_rt<E, S, 0u, 0u>(v, t, rank, 1 << (j - LOCAL), (rank >> (j - LOCAL)) & 1, cur);
+            cta_layer_rt<E, S, 0u, 0u, LIVE, UA>(v, t, rank, 1 << (j - LOCAL), (rank >> (j - LOCAL)) & 1, cur);
         // merges inside the CTA: warp and lane bits at run time, then registers
 #pragma unroll 1
         for (int j = LOCAL - 1; j >= S::LK; --j) {
-            if constexpr (SB) cross_layer_rt<E, S, 0u>(v, t, j, cur, nxt, CtaBarrierSingle{});
-            else cross_layer_rt<E, S, 0u>(v, t, j, cur, nxt, CtaBarrier{});
+            if constexpr (SB) cross_layer_rt<E, S, 0u, LIVE, UA>(v, t, j, cur, nxt, CtaBarrierSingle{});
+            else cross_layer_rt<E, S, 0u, LIVE, UA>(v, t, j, cur, nxt, CtaBarrier{});
         }
-        sfor<0, S::LK>([&](auto jc) {
-            constexpr int j = S::LK - 1 - decltype(jc)::value;
-            layer<E, S, (1u << j)>(v, t, cur, nxt, CtaBarrier{});
-        });
+        if constexpr (LIVE) {
+            sfor<0, S::LK>([&](auto jc) {
+                constexpr int j = S::LK - 1 - decltype(jc)::value;
+                layer<E, S, (1u << j)>(v, t, cur, nxt, CtaBarrier{});
+            });
+        }
     }
 }
 
+// n: the array's length.  The compact form gives warps of padding the copy
+// that only publishes and synchronises, and runs arrays without such warps
+// through the copy with aligned barriers; the unrolled form, kept for int32
+// keys, runs every warp through the whole network.
 template <class E, class S, int LC, bool SB>
 __device__ __forceinline__ void cluster_network(typename E::Reg (&v)[S::K], const int t, const int rank,
-                                                typename E::Reg*& cur, typename E::Reg*& nxt) {
+                                                typename E::Reg*& cur, typename E::Reg*& nxt, const long long n) {
     if constexpr (use_compact<E, S>()) {
-        cluster_network_compact<E, S, LC, SB>(v, t, rank, cur, nxt);
+        constexpr long long kLastWarp = (long long)((1 << LC) - 1) * S::W;
+        if (warp_live<S>(S::TPA - 1, n, kLastWarp)) cluster_network_compact<E, S, LC, SB, true, false>(v, t, rank, cur, nxt);
+        else if (warp_live<S>(t, n, (long long)rank * S::W)) cluster_network_compact<E, S, LC, SB, true, true>(v, t, rank, cur, nxt);
+        else cluster_network_compact<E, S, LC, SB, false, true>(v, t, rank, cur, nxt);
     } else {
         constexpr int LOGW = S::LOGW + LC;
         sfor<0, LOGW>([&](auto sc) {
@@ -158,7 +182,7 @@ __global__ void __launch_bounds__(S::TPA, MINB) k_sort_cluster(const typename E:
         const int base = rank * S::W + t * S::K;
         R v[S::K];
         load_tile<E, S::K>(v, in + start, base, na);
-        cluster_network<E, S, LC, SB>(v, t, rank, cur, nxt);
+        cluster_network<E, S, LC, SB>(v, t, rank, cur, nxt, na);
         store_tile<E, S::K>(v, out + start, base, na);
     }
 }

@@ -39,19 +39,27 @@ __device__ __forceinline__ void sfor(F&& f) {
 // Barrier over the threads that share one array's shared-memory tile: the
 // whole CTA when an array owns its CTA, or a named barrier when several
 // multi-warp teams share a CTA (ids 1..15; id 0 is __syncthreads).
+// unaligned(): the same barrier for warps that reach it from different code
+// (barrier.sync without .aligned): the compact network runs warps of padding
+// through a copy of the layer sequence that only publishes and synchronises.
 struct CtaBarrier {
     __device__ __forceinline__ void operator()() const { __syncthreads(); }
+    __device__ __forceinline__ void unaligned() const { asm volatile("barrier.sync 0;" ::: "memory"); }
 };
 // __syncthreads with one shared-memory buffer (see single_buffer below).
 struct CtaBarrierSingle {
     static constexpr bool kSingleBuffer = true;
     __device__ __forceinline__ void operator()() const { __syncthreads(); }
+    __device__ __forceinline__ void unaligned() const { asm volatile("barrier.sync 0;" ::: "memory"); }
 };
 struct TeamBarrier {
     int id;
     int threads;
     __device__ __forceinline__ void operator()() const {
         asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+    }
+    __device__ __forceinline__ void unaligned() const {
+        asm volatile("barrier.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
     }
 };
 // The same with one shared-memory buffer per team (see single_buffer below).
@@ -61,6 +69,9 @@ struct TeamBarrierSingle {
     int threads;
     __device__ __forceinline__ void operator()() const {
         asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+    }
+    __device__ __forceinline__ void unaligned() const {
+        asm volatile("barrier.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
     }
 };
 
@@ -195,7 +206,11 @@ __device__ __forceinline__ void lane_layer_rt(typename E::Reg (&v)[S::K], const 
     }
 }
 
-template <class E, class S, unsigned RM, class Bar>
+// LIVE == false: the copy run by a warp that holds only padding: it still
+// publishes (its partners read it) and meets every barrier, but compares
+// nothing.  Both copies take the same barriers in the same order.
+// UA: unaligned barriers, for teams whose warps run different copies.
+template <class E, class S, unsigned RM, bool LIVE, bool UA, class Bar>
 __device__ __forceinline__ void warp_layer_rt(typename E::Reg (&v)[S::K], const int t, const int tm,
                                               const bool upper, typename E::Reg*& cur, typename E::Reg*& nxt,
                                               const Bar& bar) {
@@ -204,14 +219,18 @@ __device__ __forceinline__ void warp_layer_rt(typename E::Reg (&v)[S::K], const 
         constexpr int q = decltype(qc)::value;
         cur[q * S::TPA + t] = v[q];
     });
-    bar();
-    sfor<0, S::K>([&](auto qc) {
-        constexpr int q = decltype(qc)::value;
-        const R b = cur[(q ^ int(RM)) * S::TPA + (t ^ tm)];
-        v[q] = E::pick(v[q], b, upper);
-    });
+    if constexpr (UA) bar.unaligned();
+    else bar();
+    if constexpr (LIVE) {
+        sfor<0, S::K>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            const R b = cur[(q ^ int(RM)) * S::TPA + (t ^ tm)];
+            v[q] = E::pick(v[q], b, upper);
+        });
+    }
     if constexpr (single_buffer<Bar>::value) {
-        bar();
+        if constexpr (UA) bar.unaligned();
+        else bar();
     } else {
         R* tmp = cur;
         cur = nxt;
@@ -220,35 +239,50 @@ __device__ __forceinline__ void warp_layer_rt(typename E::Reg (&v)[S::K], const 
 }
 
 // Layer with partner mask bit j >= LK (runtime j); reflection when RM != 0.
-template <class E, class S, unsigned RM, class Bar>
+template <class E, class S, unsigned RM, bool LIVE, bool UA, class Bar>
 __device__ __forceinline__ void cross_layer_rt(typename E::Reg (&v)[S::K], const int t, const int j,
                                                typename E::Reg*& cur, typename E::Reg*& nxt, const Bar& bar) {
     const int tm = RM ? (2 << (j - S::LK)) - 1 : 1 << (j - S::LK);
     const bool upper = (t >> (j - S::LK)) & 1;
     if constexpr (S::LW == 0) {
-        lane_layer_rt<E, S, RM>(v, tm, upper);
+        if constexpr (LIVE) lane_layer_rt<E, S, RM>(v, tm, upper);
     } else {
-        if (j < S::LK + S::LG) lane_layer_rt<E, S, RM>(v, tm, upper);
-        else warp_layer_rt<E, S, RM>(v, t, tm, upper, cur, nxt, bar);
+        if (j < S::LK + S::LG) {
+            if constexpr (LIVE) lane_layer_rt<E, S, RM>(v, tm, upper);
+        } else {
+            warp_layer_rt<E, S, RM, LIVE, UA>(v, t, tm, upper, cur, nxt, bar);
+        }
     }
 }
 
-template <class E, class S, class Bar>
+// LIVE == false is the copy for a warp of a multi-warp team whose elements
+// are all padding (index >= n).  Padding is the maximum element and never
+// moves, so every comparator among padding elements is a no-op and every
+// comparator of a real element with padding leaves both in place: such a
+// warp skips all its register and lane layers and only takes part in the
+// shared-memory exchanges (publish + the same barriers in the same order).
+// The output is unchanged, bit for bit.  UA: the team's warps run different
+// copies, so its barriers are the unaligned form; a team without padding
+// warps runs the LIVE copy with the aligned barriers.
+template <class E, class S, bool LIVE, bool UA, class Bar>
 __device__ __forceinline__ void network_compact(typename E::Reg (&v)[S::K], const int t, typename E::Reg*& cur,
                                                 typename E::Reg*& nxt, const Bar& bar) {
     constexpr int LK = S::LK;
     // stages inside the registers: unrolled
-    sfor<0, (LK < S::LOGW ? LK : S::LOGW)>([&](auto sc) { stage<E, S, decltype(sc)::value>(v, t, cur, nxt, bar); });
+    if constexpr (LIVE)
+        sfor<0, (LK < S::LOGW ? LK : S::LOGW)>([&](auto sc) { stage<E, S, decltype(sc)::value>(v, t, cur, nxt, bar); });
 #pragma unroll 1
     for (int st = LK; st < S::LOGW; ++st) {
-        cross_layer_rt<E, S, unsigned(S::K - 1)>(v, t, st, cur, nxt, bar);  // reflection
+        cross_layer_rt<E, S, unsigned(S::K - 1), LIVE, UA>(v, t, st, cur, nxt, bar);  // reflection
 #pragma unroll 1
-        for (int j = st - 1; j >= LK; --j) cross_layer_rt<E, S, 0u>(v, t, j, cur, nxt, bar);
+        for (int j = st - 1; j >= LK; --j) cross_layer_rt<E, S, 0u, LIVE, UA>(v, t, j, cur, nxt, bar);
         // merges 2^(LK-1) .. 1 inside the registers
-        sfor<0, LK>([&](auto jc) {
-            constexpr int j = LK - 1 - decltype(jc)::value;
-            layer<E, S, (1u << j)>(v, t, cur, nxt, bar);
-        });
+        if constexpr (LIVE) {
+            sfor<0, LK>([&](auto jc) {
+                constexpr int j = LK - 1 - decltype(jc)::value;
+                layer<E, S, (1u << j)>(v, t, cur, nxt, bar);
+            });
+        }
     }
 }
 
@@ -262,13 +296,33 @@ constexpr bool use_compact() {
     return E::kCompact && S::LOGW > S::LK;
 }
 
-// Sort the W-element tile held by the TPA threads of one array.
+// Whether the warp of team thread t holds any element below n: false only
+// for whole warps of padding in a team of whole warps (teams smaller than a
+// warp share it with other arrays and always count as live).
+template <class S>
+__device__ __forceinline__ bool warp_live(const int t, const long long n, const long long first = 0) {
+    if constexpr (S::LG == 5) return first + (long long)(t >> 5) * (32 * S::K) < n;
+    else return true;
+}
+
+// Sort the W-element tile held by the TPA threads of one array of n
+// elements.  The compact form runs warps of padding through the copy that
+// only publishes and synchronises (see network_compact); the unrolled form,
+// kept for int32 keys, runs every warp through the whole network.
 template <class E, class S, class Bar = CtaBarrier>
 __device__ __forceinline__ void network(typename E::Reg (&v)[S::K], const int t,
                                         typename E::Reg*& cur, typename E::Reg*& nxt,
-                                        const Bar& bar = Bar()) {
+                                        const Bar& bar = Bar(), const long long n = S::W) {
     if constexpr (use_compact<E, S>()) {
-        network_compact<E, S>(v, t, cur, nxt, bar);
+        if constexpr (S::LW <= 1) {
+            // At most two warps: a warp of padding would need n <= W/2, for
+            // which a tile of half the width is chosen.
+            network_compact<E, S, true, false>(v, t, cur, nxt, bar);
+        } else {
+            if (warp_live<S>(S::TPA - 1, n)) network_compact<E, S, true, false>(v, t, cur, nxt, bar);
+            else if (warp_live<S>(t, n)) network_compact<E, S, true, true>(v, t, cur, nxt, bar);
+            else network_compact<E, S, false, true>(v, t, cur, nxt, bar);
+        }
     } else {
         sfor<0, S::LOGW>([&](auto sc) { stage<E, S, decltype(sc)::value>(v, t, cur, nxt, bar); });
     }
@@ -363,8 +417,8 @@ __global__ void __launch_bounds__(CTA) k_sort_packed(const typename E::Mem* in,
         const long long off = (a < arrays ? a : 0) * (long long)n;
         R v[S::K];
         load_tile<E, S::K>(v, in + off, t * S::K, na);
-        if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{});
-        else network<E, S>(v, t, cur, nxt);
+        if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{}, na);
+        else network<E, S>(v, t, cur, nxt, CtaBarrier{}, na);
         store_tile<E, S::K>(v, out + off, t * S::K, na);
     }
 }
@@ -397,8 +451,8 @@ __global__ void __launch_bounds__(CTA) k_sort_packed_pf(const typename E::Mem* i
         const long long an = a + stride;
         R w[S::K];
         load_tile<E, S::K>(w, in + (an < arrays ? an : 0) * (long long)n, t * S::K, an < arrays ? n : 0);
-        if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{});
-        else network<E, S>(v, t, cur, nxt);
+        if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{}, a < arrays ? n : 0);
+        else network<E, S>(v, t, cur, nxt, CtaBarrier{}, a < arrays ? n : 0);
         if (a < arrays) store_tile<E, S::K>(v, out + a * (long long)n, t * S::K, n);
 #pragma unroll
         for (int q = 0; q < S::K; ++q) v[q] = w[q];

@@ -169,10 +169,10 @@ __device__ __forceinline__ void ragged_task(const typename E::Mem* in, typename 
     load_tile<E, S::K>(v, in + start, t * S::K, na);
     if constexpr (S::LW > 0) {
         static_assert(CTA / S::TPA <= 15, "named barrier ids");
-        if constexpr (SB) network<E, S>(v, t, cur, nxt, TeamBarrierSingle{1 + team, S::TPA});
-        else network<E, S>(v, t, cur, nxt, TeamBarrier{1 + team, S::TPA});
+        if constexpr (SB) network<E, S>(v, t, cur, nxt, TeamBarrierSingle{1 + team, S::TPA}, na);
+        else network<E, S>(v, t, cur, nxt, TeamBarrier{1 + team, S::TPA}, na);
     } else {
-        network<E, S>(v, t, cur, nxt);
+        network<E, S>(v, t, cur, nxt, CtaBarrier{}, na);
     }
     store_tile<E, S::K>(v, out + start, t * S::K, na);
 }
@@ -277,8 +277,8 @@ __global__ void __launch_bounds__(CTA) k_sort_idlist(const typename E::Mem* in, 
         }
         R v[S::K];
         load_tile<E, S::K>(v, in + start, t * S::K, na);
-        if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{});
-        else network<E, S>(v, t, cur, nxt);
+        if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{}, na);
+        else network<E, S>(v, t, cur, nxt, CtaBarrier{}, na);
         store_tile<E, S::K>(v, out + start, t * S::K, na);
     }
 }

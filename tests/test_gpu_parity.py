@@ -146,6 +146,20 @@ def test_large_arrays_and_multiwarp_tiles():
             check(dtype, 0, data, n, 3, gpu_sort(dtype, data, n, 3))
 
 
+@pytest.mark.parametrize("dtype", [bs.I32_I32, bs.U64_I32, bs.U64])
+@pytest.mark.parametrize("flags", [0, bs.STABLE])
+def test_whole_warps_of_padding_are_skipped_exactly(dtype, flags):
+    """Lengths whose tile has whole warps (and, for clusters, whole CTAs) of
+    padding: those warps run the copy of the network that only publishes and
+    synchronises.  Ties everywhere (16 distinct keys), so any moved element
+    would change the output."""
+    for n in (1100, 1500, 2049, 3000, 4097, 5000, 8193, 9000, 16385, 20000, 33000, 40000):
+        if n > bs.max_length(dtype, flags):
+            continue
+        data = workloads.make_packed(dtype, n, 5, "distinct16", seed=n + 17, extremes=True)
+        check(dtype, flags, data, n, 5, gpu_sort(dtype, data, n, 5, flags))
+
+
 @pytest.mark.parametrize("dtype", ALL)
 @pytest.mark.parametrize("flags", [0, bs.STABLE])
 def test_cluster_lengths(dtype, flags):
