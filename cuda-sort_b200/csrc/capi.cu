@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -94,8 +95,11 @@ DefaultTable build_defaults() {
                     const KernelEntry& e = reg[i];
                     if (e.dtype != d || e.stable != s || e.log2w != w) continue;
                     // Prefer the type's preferred register depth, then fewer
-                    // warps per array (fewer barriers).
+                    // warps per array (fewer barriers); among cluster tiles,
+                    // fewer CTAs per array (fewer distributed-shared-memory
+                    // exchanges: the throughput choice).
                     int score = (e.lk == preferred_lk(d) ? 1000 : 100 * e.lk) - 10 * e.lw;
+                    if (e.lc >= 0) score = 10000 - 100 * e.lc;
                     if (score > best_score) {
                         best_score = score;
                         best = int(i);
@@ -284,8 +288,44 @@ b200s_status launch_packed(int idx, int persistent, const void* in, void* out, i
     return B200S_OK;
 }
 
+// SMs of the current device (cached per device).
+int sm_count() {
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    int v = cache[dev & 63].load(std::memory_order_relaxed);
+    if (v == 0) {
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        cache[dev & 63].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
+
+// The latency choice for a few long arrays: a cluster tile of the same
+// working length with more, smaller CTAs per array, when every array's
+// cluster is resident at once.  Clusters place within GPCs, so larger
+// clusters leave SMs idle: on a 148-SM B200 (one 512-thread CTA per SM) 74
+// 2-CTA, 33 4-CTA and 15 8-CTA clusters are resident, i.e. 100 %, 89 % and
+// 81 % of the SMs; the rule allows arrays * CTAs per array up to that share.  The default cluster tile has the
+// fewest CTAs per array (fewer distributed-shared-memory exchanges, the higher
+// throughput once the batch fills the GPU); for one 65536-record array the
+// 8-CTA tile halves the work per SM (87 us against 150 us on a B200).
+int narrow_alternative(int idx, long long arrays) {
+    const auto& reg = registry();
+    const KernelEntry& e = reg[size_t(idx)];
+    if (e.lc < 0 || arrays <= 0) return idx;
+    int best = idx;
+    for (size_t i = 0; i < reg.size(); ++i) {
+        const KernelEntry& c = reg[i];
+        if (c.dtype == e.dtype && c.stable == e.stable && c.log2w == e.log2w && c.lc > reg[size_t(best)].lc &&
+            arrays * (1LL << c.lc) * 100 <= (c.lc <= 1 ? 100LL : c.lc == 2 ? 89LL : 81LL) * sm_count())
+            best = int(i);
+    }
+    return best;
+}
+
 int select_entry(int dtype, uint32_t flags, long long n, const b200s_tile* tile, b200s_status* st,
-                 int* persistent) {
+                 int* persistent, long long arrays = -1) {
     const int stable = effective_stable(dtype, flags);
     int idx;
     *persistent = 0;
@@ -306,6 +346,7 @@ int select_entry(int dtype, uint32_t flags, long long n, const b200s_tile* tile,
             *st = set_error(B200S_ERR_UNSUPPORTED, "array length exceeds the largest compiled tile");
             return -1;
         }
+        idx = narrow_alternative(idx, arrays);
     }
     *st = B200S_OK;
     return idx;
@@ -458,7 +499,7 @@ b200s_status b200s_sort_packed(b200s_dtype dtype, const void* d_in, void* d_out,
     if (!d_in || !d_out) return set_error(B200S_ERR_INVALID_ARGUMENT, "null buffer");
     b200s_status st;
     int persistent = 0;
-    const int idx = select_entry(dtype, flags, n, tile, &st, &persistent);
+    const int idx = select_entry(dtype, flags, n, tile, &st, &persistent, arrays);
     if (idx < 0) return st;
     return launch_packed(idx, persistent, d_in, d_out, n, arrays, static_cast<cudaStream_t>(stream));
 }

@@ -18,6 +18,12 @@ void register_cluster_rec(std::vector<KernelEntry>& o) {
     o.push_back(ClusterTile<ElemRecI32, 4, 5, 5, 0, true>::entry(1));
     o.push_back(ClusterTile<ElemRecI32, 4, 5, 5, 1, true>::entry(1));
     o.push_back(ClusterTile<ElemRecI32, 4, 5, 5, 2, true>::entry(1));
+    // Latency alternatives for a few long arrays (b200s_sort_packed picks them
+    // when every array's CTAs fit on the GPU at once): 512-thread CTAs of 8192
+    // records, 2..8 per array, half the work per SM.
+    o.push_back(ClusterTile<ElemRecI32, 4, 5, 4, 1, false>::entry(1));
+    o.push_back(ClusterTile<ElemRecI32, 4, 5, 4, 2, false>::entry(1));
+    o.push_back(ClusterTile<ElemRecI32, 4, 5, 4, 3, false>::entry(1));
     o.push_back(ClusterTile<ElemRecI32S, 4, 5, 5, 0, true>::entry(1));
     o.push_back(ClusterTile<ElemRecI32S, 4, 5, 5, 1, true>::entry(1));
     o.push_back(ClusterTile<ElemRecI32S, 4, 5, 5, 2, true>::entry(1));

@@ -120,6 +120,14 @@ struct ElemI32 {
     }
 };
 
+// int32 keys through the compact network: for the 4- and 8-CTA cluster tiles,
+// whose fully unrolled network spills at 128 registers (432-728 bytes); the
+// compact form does not, and is 5-8 % faster there (16 M keys, n = 65536:
+// 0.43 -> 0.40 ms; 131072: 0.61 -> 0.58 ms).  Same comparators, same output.
+struct ElemI32C : ElemI32 {
+    static constexpr bool kCompact = true;
+};
+
 // ---- uint64 keys -------------------------------------------------------------
 struct ElemU64 {
     using Mem = uint64_t;

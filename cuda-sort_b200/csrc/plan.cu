@@ -143,8 +143,10 @@ int overflow_entries(int dtype, int stable, int first_log2w, int* idx) {
     for (int w = first_log2w; n < kMaxOverflow; ++w, ++n) {
         int found = -1;
         const auto& reg = registry();
+        // the cluster tile with the fewest CTAs per array (throughput)
         for (size_t i = 0; i < reg.size(); ++i)
-            if (reg[i].dtype == dtype && reg[i].stable == stable && reg[i].lc >= 0 && reg[i].log2w == w)
+            if (reg[i].dtype == dtype && reg[i].stable == stable && reg[i].lc >= 0 && reg[i].log2w == w &&
+                (found < 0 || reg[i].lc < reg[size_t(found)].lc))
                 found = int(i);
         if (found < 0) break;
         if (idx) idx[n] = found;
