@@ -369,6 +369,8 @@ const char* b200s_status_string(b200s_status s) {
         case B200S_ERR_OUT_OF_MEMORY: return "out of memory";
         case B200S_ERR_TIMEOUT: return "timeout";
         case B200S_ERR_BUDGET: return "over budget";
+        case B200S_ERR_BUSY: return "busy";
+        case B200S_ERR_CANCELLED: return "cancelled";
     }
     return "unknown status";
 }

@@ -76,21 +76,6 @@ const RaggedEntry* ragged_entry(int dtype, int stable) {
     return nullptr;
 }
 
-// Cluster kernels for working lengths above the persistent kernel's range.
-int cluster_buckets(int dtype, int stable, int first_log2w, int* idx) {
-    int n = 0;
-    for (int w = first_log2w; n < kMaxOverflow; ++w, ++n) {
-        int found = -1;
-        const auto& reg = registry();
-        for (size_t i = 0; i < reg.size(); ++i)
-            if (reg[i].dtype == dtype && reg[i].stable == stable && reg[i].lc >= 0 && reg[i].log2w == w)
-                found = int(i);
-        if (found < 0) break;
-        idx[n] = found;
-    }
-    return n;
-}
-
 }  // namespace
 }  // namespace b200s
 
@@ -127,7 +112,7 @@ extern "C" b200s_status b200s_sort_ragged_noalloc(b200s_dtype dtype, uint32_t fl
     int cluster_idx[kMaxOverflow] = {};
     spec.nb = rk->nb;
     spec.over_lo = kRaggedLmin + rk->nb;
-    spec.n_over = cluster_buckets(dtype, stable, spec.over_lo, cluster_idx);
+    spec.n_over = overflow_entries(dtype, stable, spec.over_lo, cluster_idx);
     spec.stride = kNoAllocArrays;
 
     cudaStream_t cs = static_cast<cudaStream_t>(stream);

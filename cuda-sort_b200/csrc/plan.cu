@@ -130,20 +130,16 @@ b200s_status record_sequence(b200s_plan* p, const void* in, void* out, const int
 
 }  // namespace
 
-extern "C" {
-
-}  // extern "C"
-
-namespace {
+namespace b200s {
 
 // Cluster kernels that extend the persistent kernel's range: consecutive
-// working lengths above its largest bucket.  Returns the number found.
+// working lengths above its largest bucket, each the cluster tile with the
+// fewest CTAs per array (the throughput tile).  Returns the number found.
 int overflow_entries(int dtype, int stable, int first_log2w, int* idx) {
     int n = 0;
     for (int w = first_log2w; n < kMaxOverflow; ++w, ++n) {
         int found = -1;
         const auto& reg = registry();
-        // the cluster tile with the fewest CTAs per array (throughput)
         for (size_t i = 0; i < reg.size(); ++i)
             if (reg[i].dtype == dtype && reg[i].stable == stable && reg[i].lc >= 0 && reg[i].log2w == w &&
                 (found < 0 || reg[i].lc < reg[size_t(found)].lc))
@@ -154,7 +150,7 @@ int overflow_entries(int dtype, int stable, int first_log2w, int* idx) {
     return n;
 }
 
-}  // namespace
+}  // namespace b200s
 
 extern "C" {
 

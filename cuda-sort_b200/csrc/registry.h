@@ -78,4 +78,12 @@ void register_ragged_u64(std::vector<RaggedEntry>& out);
 
 const std::vector<RaggedEntry>& ragged_registry();
 
+// Registry indices of the cluster kernels that sort the ragged working lengths
+// first_log2w, first_log2w + 1, ... above the persistent kernel's buckets (at
+// most kMaxOverflow of them; idx may be null): for each length the cluster
+// tile with the fewest CTAs per array.  Returns how many lengths are covered.
+// Plans and the allocation-free ragged sort both use it, so they run the same
+// kernels.
+int overflow_entries(int dtype, int stable, int first_log2w, int* idx);
+
 }  // namespace b200s

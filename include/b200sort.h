@@ -188,8 +188,13 @@ int32_t b200s_plan_plain_launches(const b200s_plan* plan);
  *     (different streams, different host threads) race and corrupt each
  *     other; order them on one stream;
  *   - the first call on each device looks up the scratch's device address and
- *     sets kernel attributes; make that first call before any stream capture.
- * It calls no cudaMalloc or cudaFree. */
+ *     sets kernel attributes; make that first call before any stream capture;
+ *   - that address is kept for the life of the process: after a
+ *     cudaDeviceReset of a device this entry point must not be called on it
+ *     again (the reset reloads the library's device code elsewhere).
+ * It runs the same kernels as b200s_sort_ragged (including the same cluster
+ * tile for arrays above the persistent kernel's range) and calls no
+ * cudaMalloc or cudaFree. */
 #define B200S_NOALLOC_MAX_ARRAYS 32768
 b200s_status b200s_sort_ragged_noalloc(b200s_dtype dtype, uint32_t flags, const void* d_in, void* d_out,
                                        const int32_t* d_offsets, int64_t arrays, void* stream);

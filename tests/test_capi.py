@@ -33,8 +33,11 @@ def test_every_declared_symbol_is_exported():
 
 def test_version_and_status_strings():
     assert "sm_100a" in bs.version()
-    for s in range(7):
-        assert bs.lib().b200s_status_string(s)
+    # every value of b200s_status has its own string
+    strings = [bs.lib().b200s_status_string(s) for s in range(9)]
+    assert all(strings) and b"unknown status" not in strings
+    assert len(set(strings)) == 9
+    assert bs.lib().b200s_status_string(99) == b"unknown status"
 
 
 @pytest.mark.parametrize("args,status", [

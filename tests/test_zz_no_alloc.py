@@ -67,6 +67,23 @@ def test_noalloc_matches_plan_on_two_calls_in_a_row(dtype, flags):
     assert np.array_equal(free2, plan2)
 
 
+@pytest.mark.parametrize("dtype", [bs.I32_I32, bs.U64_I32])
+def test_noalloc_long_arrays_take_the_plans_cluster_tiles(dtype):
+    # arrays of 16385 .. 65536 records reach the largest cluster buckets; both
+    # paths must run the same tile there, so outputs (tie order included)
+    # match and the no-alloc call is not slower than the plan's
+    top = bs.ragged_max_length(dtype, 0)
+    assert top >= 65536
+    rng = np.random.default_rng(303)
+    lengths = np.concatenate([rng.integers(32769, 65537, size=6), rng.integers(16385, 32769, size=4),
+                              rng.integers(1, 3000, size=40)])
+    rng.shuffle(lengths)
+    data, off = workloads.make_ragged(dtype, lengths, "distinct16", seed=303, extremes=True)
+    for _ in range(2):
+        plan, free = _run_both(dtype, 0, data, off)
+        assert np.array_equal(free, plan)
+
+
 def test_noalloc_rejects_batches_beyond_its_capacity():
     fn = _noalloc()
     rc = fn(bs.I32, 0, 16, 16, 16, MAX_ARRAYS + 1, 0)
