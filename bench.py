@@ -85,9 +85,9 @@ def parse():
                     help="packed workloads: skip the plain-form, CUB and reference-V6 timings")
     ap.add_argument("--preroll", type=float, default=1.5,
                     help="seconds of untimed sorting before the timed region, so clocks settle")
-    ap.add_argument("--form", default="table", choices=["table", "0", "1", "2"],
+    ap.add_argument("--form", default="table", choices=["table", "0", "1", "2", "3"],
                     help="packed workloads: launch form of the tabled tile (0 one-shot, 1 register prefetch, "
-                         "2 TMA pipeline); 'table' uses the tile table's choice")
+                         "2 TMA pipeline, 3 transposed network); 'table' uses the tile table's choice")
     ap.add_argument("--tile", default=None, help="packed workloads: tile shape log2_items,log2_lanes,log2_warps "
                                                   "instead of the table's")
     ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds per rate point")
@@ -123,11 +123,14 @@ def layer_counts(lk, lg, lw, lc=0):
 ALU_PER_ELEM = {bs.I32: (1.0, 2.0), bs.I32_I32: (2.5, 5.0), bs.U64: (2.5, 5.0), bs.U64_I32: (2.5, 5.0)}
 
 
-def alu_roofline(dtype, tile, elements, seconds, sm_mhz):
+def alu_roofline(dtype, tile, elements, seconds, sm_mhz, form=0):
     """Integer-ALU bound of the network: modelled instructions per element x
     element slots over the B200's ALU rate (16 lanes per clock per SM
-    sub-partition, 4 per SM, 148 SMs)."""
+    sub-partition, 4 per SM, 148 SMs).  Launch form 3 (the transposed network)
+    runs every layer inside one thread's registers."""
     reg, lane, warp, cta = layer_counts(tile.log2_items, tile.log2_lanes, tile.log2_warps, tile.log2_ctas)
+    if form == 3:
+        reg, lane, warp = reg + lane + warp, 0, 0
     inside, across = ALU_PER_ELEM[dtype]
     per_elem = reg * inside + (lane + warp + cta) * across
     sms = 148
@@ -596,7 +599,9 @@ def run_gpu(args, wl):
         keys_in = data if dtype in (bs.I32, bs.U64) else data["key"]
         keys_out = got if dtype in (bs.I32, bs.U64) else got["key"]
         verified = bool(np.array_equal(keys_out.reshape(arrays, n), np.sort(keys_in.reshape(arrays, n), axis=1)))
-        kernel = {0: "k_sort_packed", 1: "k_sort_packed_pf", 2: "k_sort_packed_tma"}[form]
+        if form == 3 and not bs.tile_info(dtype, n, flags, eff).xpose_form:
+            form = 0
+        kernel = {0: "k_sort_packed", 1: "k_sort_packed_pf", 2: "k_sort_packed_tma", 3: "k_sort_xpose"}[form]
         launches = args.steps
         if ctx.world == 1 and not args.no_baselines:
             extra["baselines"] = gpu_baselines(ctx, wl, data, host, eff)
@@ -643,7 +648,7 @@ def run_gpu(args, wl):
     t_hbm = algo_bytes / (hbm * 1e9)
     if wl["kind"] == "packed":
         w = 1 << (eff.log2_items + eff.log2_lanes + eff.log2_warps + eff.log2_ctas)
-        roofline["alu"] = alu_roofline(dtype, eff, wl["arrays"] * w, ms_step * 1e-3, clocks.get("sm_mhz"))
+        roofline["alu"] = alu_roofline(dtype, eff, wl["arrays"] * w, ms_step * 1e-3, clocks.get("sm_mhz"), form)
         wmin = 1 << max(5, int(wl["n"] - 1).bit_length())
         roofline["onchip"] = onchip_roofline(np.full(wl["arrays"], wmin), bs.ELEM_BYTES[dtype], ms_step * 1e-3,
                                              t_hbm, ctx.local, lc=eff.log2_ctas, arrays=wl["arrays"])

@@ -59,14 +59,15 @@ class Tile(ctypes.Structure):
                     self.log2_ctas)
 
     def with_form(self, form):
-        """The same shape with launch form 0 (one-shot), 1 (register prefetch) or 2 (TMA pipeline)."""
+        """The same shape with launch form 0 (one-shot), 1 (register prefetch), 2 (TMA pipeline) or 3
+        (transposed network)."""
         return Tile(self.log2_items, self.log2_lanes, self.log2_warps, self.cta_threads, form, self.log2_ctas)
 
 
 class TileInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int32) for n in ("registers_per_thread", "local_bytes_per_thread", "shared_bytes",
                                               "cta_threads", "active_ctas_per_sm", "working", "arrays_per_cta",
-                                              "tma_form")]
+                                              "tma_form", "xpose_form")]
 
 
 class ServerConfig(ctypes.Structure):

@@ -17,6 +17,7 @@
 
 #include "b200sort.h"
 #include "registry.h"
+#include "xpose_registry.h"
 
 namespace b200s {
 
@@ -217,9 +218,9 @@ b200s_status parse_table_file(const char* path, TableRows* out) {
         if (idx < 0 || registry()[size_t(idx)].log2w < w)
             return set_error(B200S_ERR_UNSUPPORTED,
                              "tile table line " + std::to_string(lineno) + ": tile not compiled or too short");
-        if (pers < 0 || pers > 2)
+        if (pers < 0 || pers > 3)
             return set_error(B200S_ERR_INVALID_ARGUMENT,
-                             "tile table line " + std::to_string(lineno) + ": launch form must be 0, 1 or 2");
+                             "tile table line " + std::to_string(lineno) + ": launch form must be 0 .. 3");
         out->packed.push_back({d * 2 + stable, w, idx, pers});
     }
     return B200S_OK;
@@ -266,12 +267,29 @@ const TmaEntry* tma_for(const KernelEntry& e, const void* in, const void* out, i
     return nullptr;
 }
 
+// The transposed-network kernel (launch form 3) for registry entry e, or null
+// when none is compiled for its shape.
+const XposeEntry* xpose_for(const KernelEntry& e) {
+    if (e.lw != 0 || e.lc >= 0) return nullptr;
+    for (const XposeEntry& x : xpose_registry())
+        if (x.dtype == e.dtype && x.stable == e.stable && x.lk == e.lk && x.lg == e.lg) return &x;
+    return nullptr;
+}
+
 // Launch the packed kernel of registry entry `idx`: form 0 one-shot, 1
-// persistent with register prefetch, 2 persistent TMA pipeline (form 0 when
-// the batch does not qualify).
+// persistent with register prefetch, 2 persistent TMA pipeline, 3 transposed
+// network (form 0 when the batch or the tile does not qualify).
 b200s_status launch_packed(int idx, int persistent, const void* in, void* out, int n,
                            long long arrays, cudaStream_t st) {
     const KernelEntry& e = registry()[size_t(idx)];
+    if (persistent == 3) {
+        if (const XposeEntry* x = xpose_for(e)) {
+            const cudaError_t err = x->launch(in, out, n, arrays, st);
+            if (err != cudaSuccess) return cuda_error(err, "transposed-network sort kernel launch");
+            return B200S_OK;
+        }
+        persistent = 0;
+    }
     if (persistent == 2) {
         if (const TmaEntry* t = tma_for(e, in, out, n, arrays)) {
             const cudaError_t err = t->launch(in, out, n, arrays, st);
@@ -330,7 +348,7 @@ int select_entry(int dtype, uint32_t flags, long long n, const b200s_tile* tile,
     int idx;
     *persistent = 0;
     if (tile) {
-        *persistent = tile->persistent < 0 ? 0 : (tile->persistent > 2 ? 2 : tile->persistent);
+        *persistent = tile->persistent < 0 ? 0 : (tile->persistent > 3 ? 3 : tile->persistent);
         idx = lookup_tile(dtype, stable, *tile);
         if (idx < 0) {
             *st = set_error(B200S_ERR_UNSUPPORTED, "no compiled kernel for the requested tile");
@@ -457,6 +475,7 @@ b200s_status b200s_tile_info_get(b200s_dtype dtype, uint32_t flags, const b200s_
     out->arrays_per_cta = e.lc >= 0 ? 0 : e.apc;
     static const char aligned[16] = {};  // any 16-byte aligned address stands for the buffers
     out->tma_form = tma_for(e, aligned, aligned, std::max(1, n), 1) ? 1 : 0;
+    out->xpose_form = xpose_for(e) ? 1 : 0;
     return B200S_OK;
 }
 

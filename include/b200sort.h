@@ -87,7 +87,10 @@ typedef struct b200s_tile {
                             into registers; 2: persistent CTAs streaming chunks of arrays
                             through shared memory with TMA loads and stores (used when every
                             array is whole 128-byte rows, at most 256, and the buffers are
-                            16-byte aligned; form 0 otherwise) */
+                            16-byte aligned; form 0 otherwise); 3: transposed network, every
+                            comparator layer in registers with the tile re-laid out through
+                            shared memory between register windows (single-warp int32-key
+                            tiles of 32 keys per lane; form 0 for other tiles) */
     int32_t log2_ctas;   /* CTAs per array: 0 for single-CTA tiles (cluster tiles of one
                             CTA exist only where no single-CTA tile of that shape does) */
 } b200s_tile;
@@ -118,6 +121,7 @@ typedef struct b200s_tile_info {
     int32_t working;        /* working length W of the tile */
     int32_t arrays_per_cta; /* 0 for cluster tiles (several CTAs per array) */
     int32_t tma_form;       /* 1 if launch form 2 runs a TMA kernel for this tile and n */
+    int32_t xpose_form;     /* 1 if launch form 3 runs a transposed-network kernel for this tile */
 } b200s_tile_info;
 b200s_status b200s_tile_info_get(b200s_dtype dtype, uint32_t flags, const b200s_tile* tile, int32_t n,
                                  b200s_tile_info* out);
