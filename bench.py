@@ -90,6 +90,11 @@ def parse():
                          "2 TMA pipeline, 3 transposed network); 'table' uses the tile table's choice")
     ap.add_argument("--tile", default=None, help="packed workloads: tile shape log2_items,log2_lanes,log2_warps "
                                                   "instead of the table's")
+    ap.add_argument("--distribution", default=None, choices=list(workloads.DISTRIBUTIONS),
+                    help="packed workloads: key distribution instead of the workload's (uniform)")
+    ap.add_argument("--sorted-check", action="store_true",
+                    help="packed workloads: B200S_SORTED_CHECK (test each array first, skip it when in order); "
+                         "the reference-V6 baseline then runs with Sorted=true")
     ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds per rate point")
     ap.add_argument("--rates", default="1e4,3e4,1e5,3e5,1e6", help="serving: Poisson arrival rates (req/s)")
     return ap.parse_args()
@@ -304,7 +309,8 @@ def make_input(wl, seed):
 def config_of(args, wl, data):
     c = {"workload": args.workload, "kind": wl["kind"], "arrays_per_gpu": wl["arrays"],
          "key_dtype": DTYPE_NAMES[wl["dtype"]], "distribution": wl["dist"],
-         "stable": bool(wl["flags"] & bs.STABLE), "parallelism": "replicas (arrays are independent)",
+         "stable": bool(wl["flags"] & bs.STABLE), "sorted_check": bool(wl["flags"] & bs.SORTED_CHECK),
+         "parallelism": "replicas (arrays are independent)",
          "keys_per_gpu": int(len(data))}
     if wl["kind"] == "packed":
         c["n"] = wl["n"]
@@ -508,7 +514,8 @@ def gpu_baselines(ctx, wl, data, host, ours_tile):
     family("ours", [(repr(ours_tile), lambda p: bs.sort_packed_status(dtype, p, p, n, arrays, flags, ours_tile, st))])
     plain = ours_tile.with_form(0)
     family("plain", [(repr(plain), lambda p: bs.sort_packed_status(dtype, p, p, n, arrays, flags, plain, st))])
-    if dtype in (bs.I32, bs.I32_I32) and not flags and os.path.exists(CUB_LIB) and w <= 4096:
+    plain_flags = flags & ~bs.SORTED_CHECK
+    if dtype in (bs.I32, bs.I32_I32) and not plain_flags and os.path.exists(CUB_LIB) and w <= 4096:
         cub = ctypes.CDLL(CUB_LIB)
         cub.cub_block_merge_sort.restype = ctypes.c_int
         cub.cub_block_merge_sort.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
@@ -516,7 +523,7 @@ def gpu_baselines(ctx, wl, data, host, ours_tile):
         family("cub", [("threads=%d items=%d" % (th, w // th),
                         lambda p, th=th: cub.cub_block_merge_sort(dtype, p, n, arrays, w, th, st))
                        for th in (32, 64, 128, 256, 512, 1024) if th <= w and w // th <= 32])
-    if dtype in (bs.I32, bs.I32_I32) and not flags:
+    if dtype in (bs.I32, bs.I32_I32) and not plain_flags:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import cpu_oracle as orc
         if orc.ref_gpu_available() and w <= (4096 if dtype == bs.I32 else 2048):
@@ -526,7 +533,11 @@ def gpu_baselines(ctx, wl, data, host, ours_tile):
             for th in (32, 64, 128, 256, 512, 1024):
                 if th > w or w // th > 16:
                     continue
-                for so, sh, asy in ((0, 0, 0), (0, 1, 0), (0, 0, 1), (0, 1, 1), (1, 0, 0)):
+                # with the sortedness check, the reference's own Sorted switch (Sorted=true
+                # compiles with Shared=Async=false only in its sweep)
+                combos = ((1, 0, 0),) if flags & bs.SORTED_CHECK else ((0, 0, 0), (0, 1, 0), (0, 0, 1), (0, 1, 1),
+                                                                        (1, 0, 0))
+                for so, sh, asy in combos:
                     cands.append(("threads=%d sorted=%d shared=%d async=%d" % (th, so, sh, asy),
                                   lambda p, th=th, so=so, sh=sh, asy=asy: fn(p, n, arrays, w, th, so, sh, asy, st)))
             family("ref_v6", cands)
@@ -822,7 +833,11 @@ def run_serving(args, wl):
 
 def main():
     args = parse()
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
+    if args.distribution and wl["kind"] == "packed":
+        wl["dist"] = args.distribution
+    if args.sorted_check and wl["kind"] == "packed":
+        wl["flags"] = wl["flags"] | bs.SORTED_CHECK
     if args.impl == "reference":
         return reference_arm(args, wl)
     if wl["kind"] == "serving":

@@ -278,13 +278,17 @@ const XposeEntry* xpose_for(const KernelEntry& e) {
 
 // Launch the packed kernel of registry entry `idx`: form 0 one-shot, 1
 // persistent with register prefetch, 2 persistent TMA pipeline, 3 transposed
-// network (form 0 when the batch or the tile does not qualify).
+// network (form 0 when the batch or the tile does not qualify).  opts:
+// kOptSortedCheck (the sortedness test of B200S_SORTED_CHECK) is run by forms
+// 0, 1 and 3; a form-2 request with it runs form 0, and the cluster kernels
+// ignore it.
 b200s_status launch_packed(int idx, int persistent, const void* in, void* out, int n,
-                           long long arrays, cudaStream_t st) {
+                           long long arrays, cudaStream_t st, unsigned opts = 0) {
     const KernelEntry& e = registry()[size_t(idx)];
+    if (persistent == 2 && (opts & kOptSortedCheck)) persistent = 0;
     if (persistent == 3) {
         if (const XposeEntry* x = xpose_for(e)) {
-            const cudaError_t err = x->launch(in, out, n, arrays, st);
+            const cudaError_t err = x->launch(in, out, n, arrays, st, opts);
             if (err != cudaSuccess) return cuda_error(err, "transposed-network sort kernel launch");
             return B200S_OK;
         }
@@ -300,8 +304,8 @@ b200s_status launch_packed(int idx, int persistent, const void* in, void* out, i
     }
     long long grid = (arrays + e.apc - 1) / e.apc;
     grid = std::min<long long>(grid, 0x7fffffffLL);
-    cudaError_t err = persistent ? e.launch_pf(in, out, n, arrays, grid, st)
-                                 : e.launch(in, out, n, arrays, grid, st);
+    cudaError_t err = persistent ? e.launch_pf(in, out, n, arrays, grid, st, opts)
+                                 : e.launch(in, out, n, arrays, grid, st, opts);
     if (err != cudaSuccess) return cuda_error(err, "sort kernel launch");
     return B200S_OK;
 }
@@ -522,7 +526,8 @@ b200s_status b200s_sort_packed(b200s_dtype dtype, const void* d_in, void* d_out,
     int persistent = 0;
     const int idx = select_entry(dtype, flags, n, tile, &st, &persistent, arrays);
     if (idx < 0) return st;
-    return launch_packed(idx, persistent, d_in, d_out, n, arrays, static_cast<cudaStream_t>(stream));
+    return launch_packed(idx, persistent, d_in, d_out, n, arrays, static_cast<cudaStream_t>(stream),
+                         (flags & B200S_SORTED_CHECK) ? kOptSortedCheck : 0u);
 }
 
 }  // extern "C"
@@ -656,7 +661,8 @@ b200s_status b200s_sort_packed_host(b200s_session* s, b200s_dtype dtype, const v
         if (e != cudaSuccess) return drain(cuda_error(e, "session slot wait"));
         e = cudaMemcpyAsync(s->dbuf[k], src + size_t(first) * array_bytes, bytes, cudaMemcpyHostToDevice, s->in);
         if (e != cudaSuccess) return drain(cuda_error(e, "host-to-device copy"));
-        st = launch_packed(idx, persistent, s->dbuf[k], s->dbuf[k], n, count, s->in);
+        st = launch_packed(idx, persistent, s->dbuf[k], s->dbuf[k], n, count, s->in,
+                           (flags & B200S_SORTED_CHECK) ? kOptSortedCheck : 0u);
         if (st != B200S_OK) return drain(st);
         e = cudaEventRecord(s->sorted[k], s->in);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(s->out, s->sorted[k], 0);

@@ -95,6 +95,10 @@ __device__ __forceinline__ int32_t shfl_x(int32_t v, int m) {
 __device__ __forceinline__ uint64_t shfl_x(uint64_t v, int m) {
     return __shfl_xor_sync(0xffffffffu, (unsigned long long)v, m);
 }
+__device__ __forceinline__ int32_t shfl_d(int32_t v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+__device__ __forceinline__ uint64_t shfl_d(uint64_t v, int d) {
+    return __shfl_down_sync(0xffffffffu, (unsigned long long)v, d);
+}
 
 // ---- int32 keys --------------------------------------------------------------
 struct ElemI32 {
@@ -106,6 +110,9 @@ struct ElemI32 {
     static __device__ __forceinline__ Reg from_mem(Mem m, int) { return m; }
     static __device__ __forceinline__ Mem to_mem(Reg r) { return r; }
     static __device__ __forceinline__ Reg shfl(Reg v, int m) { return shfl_x(v, m); }
+    static __device__ __forceinline__ Reg shfl_down(Reg v, int d) { return shfl_d(v, d); }
+    // b belongs before a (the pair (a, b) is out of order).
+    static __device__ __forceinline__ bool after(Reg a, Reg b) { return b < a; }
     // Ascending compare-exchange of (lower, upper).  Equal keys are
     // indistinguishable, so min/max is the keep-own rule.
     static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
@@ -138,6 +145,8 @@ struct ElemU64 {
     static __device__ __forceinline__ Reg from_mem(Mem m, int) { return m; }
     static __device__ __forceinline__ Mem to_mem(Reg r) { return r; }
     static __device__ __forceinline__ Reg shfl(Reg v, int m) { return shfl_x(v, m); }
+    static __device__ __forceinline__ Reg shfl_down(Reg v, int d) { return shfl_d(v, d); }
+    static __device__ __forceinline__ bool after(Reg a, Reg b) { return b < a; }
     static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
         const Reg a = lo, b = hi;
         const bool sw = b < a;
@@ -166,6 +175,8 @@ struct ElemRecI32 {
     static __device__ __forceinline__ Reg shfl(Reg v, int m) {
         return Reg{shfl_x(v.key, m), shfl_x(v.data, m)};
     }
+    static __device__ __forceinline__ Reg shfl_down(Reg v, int d) { return Reg{shfl_d(v.key, d), shfl_d(v.data, d)}; }
+    static __device__ __forceinline__ bool after(const Reg& a, const Reg& b) { return b.key < a.key; }
     static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
         const Reg a = lo, b = hi;
         const bool sw = b.key < a.key;          // strict: ties keep their places
@@ -198,9 +209,13 @@ struct ElemRecI32S {
     static __device__ __forceinline__ Reg shfl(Reg v, int m) {
         return Reg{shfl_x(v.key, m), shfl_x(v.data, m), shfl_x(v.pos, m)};
     }
+    static __device__ __forceinline__ Reg shfl_down(Reg v, int d) {
+        return Reg{shfl_d(v.key, d), shfl_d(v.data, d), shfl_d(v.pos, d)};
+    }
     static __device__ __forceinline__ bool lt(const Reg& a, const Reg& b) {
         return a.key < b.key || (a.key == b.key && a.pos < b.pos);
     }
+    static __device__ __forceinline__ bool after(const Reg& a, const Reg& b) { return lt(b, a); }
     static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
         const Reg a = lo, b = hi;
         const bool sw = lt(b, a);
@@ -237,6 +252,8 @@ struct ElemRecU64 {
     static __device__ __forceinline__ Reg shfl(Reg v, int m) {
         return Reg{shfl_x(v.key, m), shfl_x(v.data, m)};
     }
+    static __device__ __forceinline__ Reg shfl_down(Reg v, int d) { return Reg{shfl_d(v.key, d), shfl_d(v.data, d)}; }
+    static __device__ __forceinline__ bool after(const Reg& a, const Reg& b) { return b.key < a.key; }
     // Field by field: whole-struct selects of this padded register record
     // made the compiler spill in the large tiles.
     static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
@@ -272,9 +289,13 @@ struct ElemRecU64S {
     static __device__ __forceinline__ Reg shfl(Reg v, int m) {
         return Reg{shfl_x(v.key, m), shfl_x(v.data, m), shfl_x(v.pos, m)};
     }
+    static __device__ __forceinline__ Reg shfl_down(Reg v, int d) {
+        return Reg{shfl_d(v.key, d), shfl_d(v.data, d), shfl_d(v.pos, d)};
+    }
     static __device__ __forceinline__ bool lt(const Reg& a, const Reg& b) {
         return a.key < b.key || (a.key == b.key && a.pos < b.pos);
     }
+    static __device__ __forceinline__ bool after(const Reg& a, const Reg& b) { return lt(b, a); }
     static __device__ __forceinline__ void cex(Reg& lo, Reg& hi) {
         const Reg a = lo, b = hi;
         const bool sw = lt(b, a);

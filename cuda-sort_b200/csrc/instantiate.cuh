@@ -34,12 +34,12 @@ struct Packed {
         return e;
     }
     static cudaError_t launch(const void* in, void* out, int n, long long arrays, long long grid,
-                              cudaStream_t st) {
+                              cudaStream_t st, unsigned opts) {
         auto fn = k_sort_packed<E, S, CTA, SB>;
         cudaError_t e = prepare<0>(reinterpret_cast<const void*>(fn));
         if (e != cudaSuccess) return e;
         fn<<<dim3(unsigned(grid)), dim3(CTA), SMEM, st>>>(
-            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), n, arrays);
+            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), n, arrays, opts);
         return cudaGetLastError();
     }
     static cudaError_t launch_list(const void* in, void* out, const int* off, const int* ids, int count,
@@ -55,7 +55,7 @@ struct Packed {
     // Persistent launch: as many CTAs as fit at once (cached per device), never
     // more than the batch needs.
     static cudaError_t launch_pf(const void* in, void* out, int n, long long arrays, long long grid,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, unsigned opts) {
         auto fn = k_sort_packed_pf<E, S, CTA, SB>;
         cudaError_t e = prepare<2>(reinterpret_cast<const void*>(fn));
         if (e != cudaSuccess) return e;
@@ -76,7 +76,7 @@ struct Packed {
         }
         const long long g = grid < cap ? grid : cap;
         fn<<<dim3(unsigned(g)), dim3(CTA), SMEM, st>>>(
-            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), n, arrays);
+            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), n, arrays, opts);
         return cudaGetLastError();
     }
     static cudaError_t attrs(cudaFuncAttributes* a) {
@@ -145,7 +145,8 @@ struct ClusterTile {
         return cudaLaunchKernelEx(&cfg, k_sort_cluster<E, S, LC, SB, MINB>, static_cast<const typename E::Mem*>(in),
                                   static_cast<typename E::Mem*>(out), n, arrays, off, ids, d_count);
     }
-    static cudaError_t launch(const void* in, void* out, int n, long long arrays, long long, cudaStream_t st) {
+    static cudaError_t launch(const void* in, void* out, int n, long long arrays, long long, cudaStream_t st,
+                              unsigned) {
         return run(in, out, n, arrays, nullptr, nullptr, nullptr, arrays, st);
     }
     static cudaError_t launch_list(const void* in, void* out, const int* off, const int* ids, int count,

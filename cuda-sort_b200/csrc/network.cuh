@@ -25,6 +25,7 @@
 #include <type_traits>
 
 #include "elem.cuh"
+#include "opts.h"
 
 namespace b200s {
 
@@ -389,6 +390,49 @@ __device__ __forceinline__ void store_tile(const typename E::Reg (&v)[K], typena
     }
 }
 
+// ---- sortedness check (the reference's Sorted switch) -------------------------
+// With its Sorted switch the reference tests the tile before the first stage
+// (and after every stage of span >= 16) and returns early when the tile is
+// already in order (cusort_v6.hpp:103-128, cusort.hpp:437-458).  A tile in
+// order is a fixed point of every comparator under the keep-own rule, so the
+// early return changes no output.  Padding (the maximum element after the n
+// valid ones) never breaks the order, so the whole tile is tested.
+
+template <class E, int K>
+__device__ __forceinline__ bool thread_in_order(const typename E::Reg (&v)[K]) {
+    bool ok = true;
+    sfor<0, K - 1>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        ok &= !E::after(v[q], v[q + 1]);
+    });
+    return ok;
+}
+
+// Whether the tile of team thread t (blocked layout, TPA threads) is in order.
+// The answer is uniform where the network needs it: over the CTA for a
+// multi-warp team (one array per CTA), over the warp for teams inside a warp
+// (true only when every array of the warp is in order), so that every lane
+// of a warp and every warp of a CTA takes the same branch.  cur: the team's
+// shared buffer (free before the network), used for the warp boundaries.
+template <class E, class S>
+__device__ __forceinline__ bool team_in_order(const typename E::Reg (&v)[S::K], const int t,
+                                              typename E::Reg* cur) {
+    using R = typename E::Reg;
+    bool ok = thread_in_order<E, S::K>(v);
+    const R nx = E::shfl_down(v[0], 1);  // the next lane's first element
+    const bool last_of_group = ((t + 1) & (S::G - 1)) == 0;
+    if (!last_of_group) ok &= !E::after(v[S::K - 1], nx);
+    if constexpr (S::LW == 0) {
+        return __all_sync(0xffffffffu, ok);
+    } else {
+        const int lane = t & 31, w = t >> 5;
+        if (lane == 0) cur[w] = v[0];
+        __syncthreads();
+        if (lane == 31 && w + 1 < (S::TPA >> 5)) ok &= !E::after(v[S::K - 1], cur[w + 1]);
+        return __syncthreads_and(ok) != 0;
+    }
+}
+
 // ---- packed batch kernel ------------------------------------------------------
 // Packed layout of the reference's batched wrappers (bench.cu:355-393):
 // array a occupies [a*n, a*n + n).  Each group of TPA threads sorts one array;
@@ -397,10 +441,12 @@ __device__ __forceinline__ void store_tile(const typename E::Reg (&v)[K], typena
 // nothing, and every warp-wide shuffle and barrier sees all its threads.
 // SB: one shared-memory buffer (two barriers per shared-memory layer, half the
 // shared memory, more CTAs per SM) instead of two.
+// opts & kOptSortedCheck: test each tile first and skip the network when it is
+// already in order (and the store too when sorting in place).
 template <class E, class S, int CTA, bool SB = false>
 __global__ void __launch_bounds__(CTA) k_sort_packed(const typename E::Mem* in,
                                                      typename E::Mem* out, int n,
-                                                     long long arrays) {
+                                                     long long arrays, unsigned opts) {
     using R = typename E::Reg;
     static_assert(CTA % S::TPA == 0, "CTA holds whole arrays");
     static_assert(S::LW == 0 || CTA == S::TPA, "a multi-warp array owns its CTA");
@@ -417,9 +463,12 @@ __global__ void __launch_bounds__(CTA) k_sort_packed(const typename E::Mem* in,
         const long long off = (a < arrays ? a : 0) * (long long)n;
         R v[S::K];
         load_tile<E, S::K>(v, in + off, t * S::K, na);
-        if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{}, na);
-        else network<E, S>(v, t, cur, nxt, CtaBarrier{}, na);
-        store_tile<E, S::K>(v, out + off, t * S::K, na);
+        const bool skip = (opts & kOptSortedCheck) && team_in_order<E, S>(v, t, cur);
+        if (!skip) {
+            if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{}, na);
+            else network<E, S>(v, t, cur, nxt, CtaBarrier{}, na);
+        }
+        if (!skip || in != out) store_tile<E, S::K>(v, out + off, t * S::K, na);
     }
 }
 
@@ -430,7 +479,7 @@ __global__ void __launch_bounds__(CTA) k_sort_packed(const typename E::Mem* in,
 template <class E, class S, int CTA, bool SB = false>
 __global__ void __launch_bounds__(CTA) k_sort_packed_pf(const typename E::Mem* in,
                                                         typename E::Mem* out, int n,
-                                                        long long arrays) {
+                                                        long long arrays, unsigned opts) {
     using R = typename E::Reg;
     constexpr int APC = CTA / S::TPA;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -451,9 +500,12 @@ __global__ void __launch_bounds__(CTA) k_sort_packed_pf(const typename E::Mem* i
         const long long an = a + stride;
         R w[S::K];
         load_tile<E, S::K>(w, in + (an < arrays ? an : 0) * (long long)n, t * S::K, an < arrays ? n : 0);
-        if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{}, a < arrays ? n : 0);
-        else network<E, S>(v, t, cur, nxt, CtaBarrier{}, a < arrays ? n : 0);
-        if (a < arrays) store_tile<E, S::K>(v, out + a * (long long)n, t * S::K, n);
+        const bool skip = (opts & kOptSortedCheck) && team_in_order<E, S>(v, t, cur);
+        if (!skip) {
+            if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{}, a < arrays ? n : 0);
+            else network<E, S>(v, t, cur, nxt, CtaBarrier{}, a < arrays ? n : 0);
+        }
+        if (a < arrays && (!skip || in != out)) store_tile<E, S::K>(v, out + a * (long long)n, t * S::K, n);
 #pragma unroll
         for (int q = 0; q < S::K; ++q) v[q] = w[q];
     }

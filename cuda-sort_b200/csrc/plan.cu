@@ -20,7 +20,7 @@ int effective_stable(int dtype, uint32_t flags);
 int ceil_log2(long long n);
 int lookup_default_entry(int dtype, int stable, long long n, int* persistent);
 b200s_status launch_packed(int idx, int persistent, const void* in, void* out, int n, long long arrays,
-                           cudaStream_t st);
+                           cudaStream_t st, unsigned opts = 0);
 
 const std::vector<RaggedEntry>& ragged_registry() {
     static std::vector<RaggedEntry> all = [] {

@@ -8,10 +8,13 @@
 #include <cstdint>
 #include <vector>
 
+#include "opts.h"
+
 namespace b200s {
 
+// opts: launch options (kOptSortedCheck in network.cuh; cluster kernels ignore them).
 using PackedLaunch = cudaError_t (*)(const void* in, void* out, int n, long long arrays,
-                                     long long grid, cudaStream_t stream);
+                                     long long grid, cudaStream_t stream, unsigned opts);
 using AttrQuery = cudaError_t (*)(cudaFuncAttributes* attr);
 // Launch over a list of array ids of a CSR batch (plain per-length launches).
 using ListLaunch = cudaError_t (*)(const void* in, void* out, const int* d_off, const int* d_ids,

@@ -21,11 +21,11 @@ struct Xpose {
     static constexpr size_t SMEM = size_t(WPC) * APW * xp_region<LK, LG>() * sizeof(typename E::Reg);
     static constexpr auto kernel() { return k_sort_xpose<E, LK, LG, WPC, MINB, STRIPED>; }
 
-    static cudaError_t launch(const void* in, void* out, int n, long long arrays, cudaStream_t st) {
+    static cudaError_t launch(const void* in, void* out, int n, long long arrays, cudaStream_t st, unsigned opts) {
         const long long per_cta = (long long)WPC * APW;
         const long long grid = std::min<long long>((arrays + per_cta - 1) / per_cta, 0x7fffffffLL);
         kernel()<<<dim3(unsigned(grid)), dim3(WPC * 32), SMEM, st>>>(
-            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), n, arrays);
+            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), n, arrays, opts);
         return cudaGetLastError();
     }
     static cudaError_t attrs(cudaFuncAttributes* a) {

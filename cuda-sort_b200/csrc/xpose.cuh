@@ -156,11 +156,38 @@ __device__ __forceinline__ void xp_reg_stage(typename E::Reg (&v)[1 << LK]) {
     });
 }
 
-// Sort the W = 2^(LK+LG) element tile of lane t (natural layout in and out).
+// Whether every array of the warp is in order (natural layout, G lanes per
+// array): warp-uniform, since the stages use full-warp synchronisation.
 template <class E, int LK, int LG>
-__device__ __forceinline__ void xp_network(typename E::Reg (&v)[1 << LK], const int t, typename E::Reg* sm) {
-    sfor<0, LK>([&](auto sc) { xp_reg_stage<E, LK, decltype(sc)::value>(v); });
-    sfor<LK, LK + LG>([&](auto sc) { xp_stage<E, LK, LG, decltype(sc)::value>(v, t, sm); });
+__device__ __forceinline__ bool xp_warp_in_order(const typename E::Reg (&v)[1 << LK], const int t) {
+    constexpr int K = 1 << LK, G = 1 << LG;
+    bool ok = thread_in_order<E, K>(v);
+    const typename E::Reg nx = E::shfl_down(v[0], 1);
+    if (t != G - 1) ok &= !E::after(v[K - 1], nx);
+    return __all_sync(0xffffffffu, ok);
+}
+
+// Sort the W = 2^(LK+LG) element tile of lane t (natural layout in and out).
+// check: the reference's Sorted switch: after every stage of span >= 16
+// (stage index >= 4) stop as soon as every array of the warp is in order.
+template <class E, int LK, int LG>
+__device__ __forceinline__ void xp_network(typename E::Reg (&v)[1 << LK], const int t, typename E::Reg* sm,
+                                           const bool check = false) {
+    bool done = false;
+    sfor<0, LK>([&](auto sc) {
+        constexpr int ST = decltype(sc)::value;
+        if (!done) {
+            xp_reg_stage<E, LK, ST>(v);
+            if (ST >= 4 && check) done = xp_warp_in_order<E, LK, LG>(v, t);
+        }
+    });
+    sfor<LK, LK + LG>([&](auto sc) {
+        constexpr int ST = decltype(sc)::value;
+        if (!done) {
+            xp_stage<E, LK, LG, ST>(v, t, sm);
+            if (check && ST + 1 < LK + LG) done = xp_warp_in_order<E, LK, LG>(v, t);
+        }
+    });
 }
 
 template <int LK, int LG>
@@ -229,7 +256,7 @@ __device__ __forceinline__ void xp_store_striped(typename E::Reg (&v)[1 << LK], 
 // previous one.  No CTA-wide barrier: every warp runs on its own.
 template <class E, int LK, int LG, int WPC, int MINB, bool STRIPED, bool PF = false>
 __global__ void __launch_bounds__(WPC * 32, MINB)
-    k_sort_xpose(const typename E::Mem* in, typename E::Mem* out, int n, long long arrays) {
+    k_sort_xpose(const typename E::Mem* in, typename E::Mem* out, int n, long long arrays, unsigned opts) {
     using R = typename E::Reg;
     constexpr int K = 1 << LK, G = 1 << LG, APW = 32 / G;
     static_assert(LG <= 5 && LG <= LK && LG >= 1, "one warp or less per array, at most two windows");
@@ -239,12 +266,25 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
     const int slot = lane >> LG, t = lane & (G - 1);
     R* sm = reinterpret_cast<R*>(smem_raw) + (warp * APW + slot) * xp_region<LK, LG>();
     const long long stride = (long long)gridDim.x * WPC * APW;
+    // With the sortedness check the tile is loaded in its own order (the
+    // striped relabelling would hide the input's order from the test).
+    const bool check = (opts & kOptSortedCheck) != 0;
     long long first = ((long long)blockIdx.x * WPC + warp) * APW;
     auto load = [&](R (&x)[K], long long a) {
         const int na = a < arrays ? n : 0;
         const typename E::Mem* src = in + (a < arrays ? a : 0) * (long long)n;
-        if constexpr (STRIPED) xp_load_striped<E, LK, LG>(x, src, t, na);
+        if (STRIPED && !check) xp_load_striped<E, LK, LG>(x, src, t, na);
         else load_tile<E, K>(x, src, t * K, na);
+    };
+    auto finish = [&](R (&x)[K], long long a) {
+        bool skip = false;
+        if (check) skip = xp_warp_in_order<E, LK, LG>(x, t);
+        if (!skip) xp_network<E, LK, LG>(x, t, sm, check);
+        if (skip && in == out) return;  // in order and in place: nothing to write
+        const int na = a < arrays ? n : 0;
+        typename E::Mem* dst = out + (a < arrays ? a : 0) * (long long)n;
+        if constexpr (STRIPED) xp_store_striped<E, LK, LG>(x, dst, t, na, sm);
+        else store_tile<E, K>(x, dst, t * K, na);
     };
     R v[K];
     if constexpr (PF) {
@@ -255,20 +295,12 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
         if constexpr (PF) {
             R w[K];
             load(w, a + stride);
-            xp_network<E, LK, LG>(v, t, sm);
-            const int na = a < arrays ? n : 0;
-            typename E::Mem* dst = out + (a < arrays ? a : 0) * (long long)n;
-            if constexpr (STRIPED) xp_store_striped<E, LK, LG>(v, dst, t, na, sm);
-            else store_tile<E, K>(v, dst, t * K, na);
+            finish(v, a);
 #pragma unroll
             for (int q = 0; q < K; ++q) v[q] = w[q];
         } else {
             load(v, a);
-            xp_network<E, LK, LG>(v, t, sm);
-            const int na = a < arrays ? n : 0;
-            typename E::Mem* dst = out + (a < arrays ? a : 0) * (long long)n;
-            if constexpr (STRIPED) xp_store_striped<E, LK, LG>(v, dst, t, na, sm);
-            else store_tile<E, K>(v, dst, t * K, na);
+            finish(v, a);
         }
     }
 }

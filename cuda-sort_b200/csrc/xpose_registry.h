@@ -12,7 +12,7 @@ struct XposeEntry {
     int dtype;
     int stable;
     int lk, lg;  // the tile shape it serves: K = 2^lk elements per lane, 2^lg lanes per array
-    cudaError_t (*launch)(const void* in, void* out, int n, long long arrays, cudaStream_t stream);
+    cudaError_t (*launch)(const void* in, void* out, int n, long long arrays, cudaStream_t stream, unsigned opts);
     cudaError_t (*attrs)(cudaFuncAttributes* attr);
     int cta;      // threads per CTA
     size_t smem;  // dynamic shared memory per CTA

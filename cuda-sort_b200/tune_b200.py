@@ -1,21 +1,26 @@
 """Autotuner for the tile table (tune/b200_table.csv, loaded by the library
 at first use from beside libb200sort.so).
 
-  python cuda-sort_b200/tune_b200.py [--out PATH] [--reps R]
+  python cuda-sort_b200/tune_b200.py [--out PATH] [--summary PATH] [--passes P]
 
 For every element type, stable flag and working length W = 2^L it times each
-compiled single-CTA tile of that W in each launch form (one slot per array /
-persistent with register prefetch / persistent TMA pipeline) on a full-length batch of about 4 M elements and
-keeps the fastest as the packed row.  For the ragged kernel it times, per
-bucket L, a batch whose lengths all fall in that bucket with the bucket's
-shape family A and with family B, and keeps the faster as the ragged row.
-Every launch starts from an L2 flushed by a 512 MB write; times are CUDA-event
-medians.  Requires a GPU.
+compiled single-CTA tile of that W in each launch form it has (0 one slot per
+array, 1 persistent with register prefetch, 2 persistent TMA pipeline, 3
+transposed network) on a full-length batch of about 4 M elements, checks the
+output, and keeps the fastest as the packed row.  For the ragged kernel it
+times, per bucket L, a batch whose lengths all fall in that bucket with the
+bucket's shape family A and with family B, and keeps the faster as the
+ragged row.
+
+Timing (devtime.batched_us): each pass evicts L2, then runs one launch on
+each of several buffer sets (at least twice the L2 in total) back to back
+between two CUDA events; the per-launch time is the median over the passes.
+Every row records the best and the runner-up with the best's spread over the
+passes; --summary writes that table as markdown.  Requires a GPU.
 """
 import argparse
 import datetime
 import os
-import statistics
 import sys
 import tempfile
 
@@ -26,59 +31,72 @@ import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
 import b200sort as bs  # noqa: E402
+import devtime  # noqa: E402
 import workloads  # noqa: E402
 
 TARGET_ELEMS = 1 << 22
+FORM_NAMES = {0: "one-shot", 1: "prefetch", 2: "TMA", 3: "transposed"}
 
 
-def timed(fn, flush, reps):
-    st = torch.cuda.current_stream()
-    times = []
-    for r in range(reps + 1):
-        flush.fill_(r & 0xFF)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        fn()
-        e1.record(st)
-        torch.cuda.synchronize()
-        if r:
-            times.append(e0.elapsed_time(e1) * 1e3)
-    return statistics.median(times)
+def _keys(dtype, arr):
+    return arr if dtype in (bs.I32, bs.U64) else arr["key"]
 
 
-def tune_packed(dtype, flags, flush, reps, log):
+def tune_packed(dtype, flags, flush, passes, log, summary):
     rows = []
     tiles = [t for t in bs.tiles(dtype, flags) if t.log2_ctas == 0 and t.cta_threads > 0]
     by_w = {}
     for t in tiles:
         by_w.setdefault(sum(t.as_tuple()), []).append(t)
+    st = torch.cuda.current_stream().cuda_stream
     for L in sorted(by_w):
         n = 1 << L
         arrays = max(1, TARGET_ELEMS // n)
         data = workloads.make_packed(dtype, n, arrays, "uniform", seed=L)
-        d_in = torch.from_numpy(data.view(np.uint8).copy()).cuda()
-        d_out = torch.empty_like(d_in)
-        st = torch.cuda.current_stream().cuda_stream
-        best = None
+        want = np.sort(_keys(dtype, data).reshape(arrays, n), axis=1).reshape(-1)
+        sets = devtime.sets_for(data.nbytes, 8)
+        src = torch.from_numpy(data.view(np.uint8).copy()).cuda()
+        ins = [src.clone() for _ in range(sets)]
+        outs = [torch.empty_like(src) for _ in range(sets)]
+        cands = []
         for base in by_w[L]:
-            forms = [base, base.with_persistent()]
-            if bs.tile_info(dtype, n, flags, base).tma_form:
-                forms.append(base.with_form(2))   # TMA pipeline, where compiled for this tile
-            for tile in forms:
-                us = timed(lambda t=tile: bs.sort_packed(dtype, d_in.data_ptr(), d_out.data_ptr(), n, arrays, flags,
-                                                         t, st), flush, reps)
-                log("packed dtype=%d flags=%d W=%d %r: %.2f us" % (dtype, flags, n, tile, us))
-                if best is None or us < best[0]:
-                    best = (us, tile)
-        t = best[1]
-        rows.append("%d,%d,%d,%d,%d,%d,%d  # %.2f us, %d arrays" % (dtype, flags, L, t.log2_items, t.log2_lanes,
-                                                                  t.log2_warps, t.persistent, best[0], arrays))
+            info = bs.tile_info(dtype, n, flags, base)
+            forms = [0, 1] + ([2] if info.tma_form else []) + ([3] if info.xpose_form else [])
+            cands += [base.with_form(f) for f in forms]
+        results = []
+        for tile in cands:
+            launches = [lambda i=i, t=tile: bs.sort_packed_status(dtype, ins[i].data_ptr(), outs[i].data_ptr(), n,
+                                                                  arrays, flags, t, st) for i in range(sets)]
+            us, spread = devtime.batched_us(launches, flush, passes)
+            if us is None:
+                continue
+            ok = bool(np.array_equal(_keys(dtype, outs[0].cpu().numpy().view(bs.NP_DTYPES[dtype])), want))
+            log("packed dtype=%d flags=%d W=%d %r: %.2f us (spread %.1f %%)%s"
+                % (dtype, flags, n, tile, us, 100 * spread, "" if ok else " WRONG OUTPUT"))
+            if ok:
+                results.append((us, spread, tile))
+        results.sort(key=lambda r: r[0])
+        (us, spread, t) = results[0]
+        second = results[1] if len(results) > 1 else None
+        tail = (", runner-up %.2f us %s" % (second[0], _shape(second[2]))) if second else ""
+        rows.append("%d,%d,%d,%d,%d,%d,%d  # %.2f us (spread %.1f %%)%s, %d arrays"
+                    % (dtype, flags, L, t.log2_items, t.log2_lanes, t.log2_warps, t.persistent, us, 100 * spread, tail,
+                       arrays))
+        summary.append(("packed", dtype, flags, n, arrays, _shape(t), us, spread,
+                        _shape(second[2]) if second else "-", second[0] if second else None))
+        del ins, outs, src
+        torch.cuda.empty_cache()
     return rows
 
 
-def tune_ragged(dtype, flags, flush, reps, log):
+def _shape(t):
+    return "K%d.G%d.W%d/%s" % (1 << t.log2_items, 1 << t.log2_lanes, 1 << t.log2_warps, FORM_NAMES[t.persistent])
+
+
+def tune_ragged(dtype, flags, flush, passes, log, summary):
     rows = []
     top = bs.ragged_max_length(dtype, flags)
+    st = torch.cuda.current_stream().cuda_stream
     L = 3
     while (1 << L) <= top:
         lo, hi = (1 << (L - 1)) + 1 if L > 3 else 1, 1 << L
@@ -86,22 +104,34 @@ def tune_ragged(dtype, flags, flush, reps, log):
         rng = np.random.default_rng(L)
         lengths = rng.integers(lo, hi, size=arrays, endpoint=True)
         data, off = workloads.make_ragged(dtype, lengths, "uniform", seed=L)
-        d_in = torch.from_numpy(data.view(np.uint8).copy()).cuda()
-        d_out = torch.empty_like(d_in)
+        sets = devtime.sets_for(data.nbytes, 6)
+        src = torch.from_numpy(data.view(np.uint8).copy()).cuda()
+        ins = [src.clone() for _ in range(sets)]
+        outs = [torch.empty_like(src) for _ in range(sets)]
         d_off = torch.from_numpy(off.astype(np.int32)).cuda()
-        st = torch.cuda.current_stream().cuda_stream
         res = {}
         for fam in (0, 1):
             with tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False) as f:
                 f.write("r,%d,%d,%d,%d\n" % (dtype, flags, L, fam))
             bs.load_tile_table(f.name)
             os.unlink(f.name)
-            with bs.Plan(dtype, arrays, flags) as plan:
-                res[fam] = timed(lambda p=plan: p.sort(d_in.data_ptr(), d_out.data_ptr(), d_off.data_ptr(), arrays, st),
-                                 flush, reps)
-            log("ragged dtype=%d flags=%d W=%d family=%d: %.2f us" % (dtype, flags, 1 << L, fam, res[fam]))
-        fam = min(res, key=res.get)
-        rows.append("r,%d,%d,%d,%d  # %.2f us vs %.2f us" % (dtype, flags, L, fam, res[fam], res[1 - fam]))
+            plans = [bs.Plan(dtype, arrays, flags) for _ in range(sets)]   # one captured graph per buffer set
+            launches = [lambda i=i: plans[i].sort(ins[i].data_ptr(), outs[i].data_ptr(), d_off.data_ptr(), arrays, st)
+                        for i in range(sets)]
+            for fn in launches:
+                fn()   # capture each plan's graph outside the timed passes
+            res[fam] = devtime.batched_us(launches, flush, passes)
+            for p in plans:
+                p.close()
+            log("ragged dtype=%d flags=%d W=%d family=%d: %.2f us (spread %.1f %%)"
+                % (dtype, flags, 1 << L, fam, res[fam][0], 100 * res[fam][1]))
+        fam = min(res, key=lambda k: res[k][0])
+        rows.append("r,%d,%d,%d,%d  # %.2f us (spread %.1f %%) vs %.2f us"
+                    % (dtype, flags, L, fam, res[fam][0], 100 * res[fam][1], res[1 - fam][0]))
+        summary.append(("ragged", dtype, flags, 1 << L, arrays, "family %s" % "AB"[fam], res[fam][0], res[fam][1],
+                        "family %s" % "AB"[1 - fam], res[1 - fam][0]))
+        del ins, outs, src
+        torch.cuda.empty_cache()
         L += 1
     # leave the process's table as tuned
     with tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False) as f:
@@ -111,28 +141,51 @@ def tune_ragged(dtype, flags, flush, reps, log):
     return rows
 
 
+def write_summary(path, summary, argv):
+    names = {bs.I32: "int32", bs.I32_I32: "int32+int32", bs.U64: "uint64", bs.U64_I32: "uint64+int32"}
+    with open(path, "w") as f:
+        f.write("# Tile table tuning on %s\n\n" % torch.cuda.get_device_name())
+        f.write("Command: `python cuda-sort_b200/tune_b200.py %s`\n\n" % " ".join(argv))
+        f.write("Per row: the fastest configuration and the runner-up, per-launch microseconds from batched CUDA "
+                "events (devtime.batched_us: L2 evicted, one launch per buffer set, median of the passes), the best's "
+                "spread over the passes, and the margin (runner-up / best - 1).\n\n")
+        f.write("| path | dtype | stable | W | arrays | best | us | spread | runner-up | us | margin |\n")
+        f.write("|---|---|---|---|---|---|---|---|---|---|---|\n")
+        for kind, d, fl, w, arrays, best, us, spread, second, us2 in summary:
+            margin = "%.1f %%" % (100 * (us2 / us - 1)) if us2 else "-"
+            f.write("| %s | %s | %s | %d | %d | %s | %.2f | %.1f %% | %s | %s | %s |\n"
+                    % (kind, names[d], "yes" if fl else "no", w, arrays, best, us, 100 * spread, second,
+                       "%.2f" % us2 if us2 else "-", margin))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(HERE, "tune", "b200_table.csv"))
-    ap.add_argument("--reps", type=int, default=7)
+    ap.add_argument("--summary", default=None, help="markdown table of best and runner-up per row")
+    ap.add_argument("--passes", type=int, default=5)
+    ap.add_argument("--only", default=None, help="comma-separated dtype codes to tune (default all)")
     args = ap.parse_args()
-    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-    lines = []
+    flush = devtime.Flusher()
+    lines, summary = [], []
     log = lambda s: print(s, flush=True)  # noqa: E731
-    for dtype in (bs.I32, bs.I32_I32, bs.U64, bs.U64_I32):
+    dtypes = [int(x) for x in args.only.split(",")] if args.only else [bs.I32, bs.I32_I32, bs.U64, bs.U64_I32]
+    for dtype in dtypes:
         for flags in ((0,) if dtype in (bs.I32, bs.U64) else (0, bs.STABLE)):
-            lines += tune_packed(dtype, flags, flush, args.reps, log)
-            lines += tune_ragged(dtype, flags, flush, args.reps, log)
+            lines += tune_packed(dtype, flags, flush, args.passes, log, summary)
+            lines += tune_ragged(dtype, flags, flush, args.passes, log, summary)
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as f:
         f.write("# b200sort tile table, written by cuda-sort_b200/tune_b200.py\n")
         f.write("# device: %s; %s; library: %s\n" % (torch.cuda.get_device_name(),
                                                      datetime.datetime.now(datetime.timezone.utc).strftime(
                                                          "%Y-%m-%d %H:%M UTC"), bs.version()))
-        f.write("# packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps,form (0 one-shot, 1 prefetch, 2 TMA)\n")
+        f.write("# packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps,form (0 one-shot, 1 prefetch, 2 TMA, "
+                "3 transposed)\n")
         f.write("# ragged rows: r,dtype,flags,log2_w,family (0: larger per-thread tile, 1: smaller)\n")
         for ln in lines:
             f.write(ln + "\n")
+    if args.summary:
+        write_summary(args.summary, summary, sys.argv[1:])
     print("wrote", args.out, len(lines), "rows")
 
 

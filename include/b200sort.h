@@ -67,8 +67,13 @@ typedef enum b200s_dtype {
 
 /* flags */
 #define B200S_STABLE 1u       /* ties keep input order (bit-exact std::stable_sort) */
-#define B200S_SORTED_CHECK 2u /* accepted for source compatibility with the reference's
-                                 `Sorted` switch; the output is identical either way   */
+#define B200S_SORTED_CHECK 2u /* the reference's `Sorted` switch (cusort_v6.hpp:103-128): the
+                                 packed path tests each array before sorting and skips the
+                                 network when it is already in order (in place: the store
+                                 too); the transposed-network form also tests after every
+                                 stage of span >= 16.  The output is identical either way.
+                                 The TMA form runs form 0 instead; the cluster and ragged
+                                 paths accept the flag and sort in full. */
 #define B200S_PLAN_NO_GRAPH 0x100u /* plan flag: launch the ragged sequence directly
                                       instead of replaying a captured CUDA graph */
 

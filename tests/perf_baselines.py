@@ -2,20 +2,22 @@
 and the reference's own V6 kernel (compiled from its headers into
 oracle/_ref/), on identical inputs.  Measurement infrastructure, not a test:
 
-  python tests/perf_baselines.py [--out FILE.json] [--reps R]
+  python tests/perf_baselines.py [--out FILE.json] [--passes P]
 
-Every timed launch starts from a freshly restored input and an L2 flushed by
-a 512 MB write, so no kernel reads a warm cache.  Times are CUDA-event
-medians per launch.  For each family the best configuration is reported:
-the reference's own sweep (bench.cu:497-521: Threads and the Sorted /
-Shared / Async switches) for V6, every thread count for CUB, every compiled
-tile for the new kernels, in each launch form.  Outputs are checked against numpy/the oracle.
+Every configuration is timed the same way (cuda-sort_b200/devtime.py): in
+place on several copies of the batch (together at least twice the 126 MB L2),
+restored from a pristine copy before each pass and then evicted from L2, one
+launch per copy back to back between two CUDA events; per-launch time = pass
+time / copies, median of the passes.  For each family the best configuration
+is reported: the reference's own sweep (bench.cu:497-521: Threads and the
+Sorted / Shared / Async switches) for V6, every thread count for CUB, every
+compiled tile in each launch form for the new kernels.  Outputs are checked
+against numpy / the oracle.
 """
 import argparse
 import ctypes
 import json
 import os
-import statistics
 import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -26,6 +28,7 @@ import torch  # noqa: E402
 
 import b200sort as bs  # noqa: E402
 import cpu_oracle as orc  # noqa: E402
+import devtime  # noqa: E402
 import workloads  # noqa: E402
 
 CUB_LIB = os.path.join(ROOT, "cuda-sort_b200", "libb200sort_cub.so")
@@ -41,30 +44,23 @@ def working(n):
 class Timer:
     def __init__(self, data):
         self.src = torch.from_numpy(data.view(np.uint8).copy()).cuda()
-        self.work = torch.empty_like(self.src)
-        self.out = torch.empty_like(self.src)
-        self.flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-        self.st = torch.cuda.current_stream()
+        self.sets = [torch.empty_like(self.src) for _ in range(devtime.sets_for(self.src.numel(), 20))]
+        self.flush = devtime.Flusher()
 
-    def time(self, launch, reps, inplace):
-        times = []
-        for r in range(reps + 2):
-            self.work.copy_(self.src)
-            self.flush.fill_(r & 0xFF)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(self.st)
-            rc = launch(self.work.data_ptr(), (self.work if inplace else self.out).data_ptr())
-            e1.record(self.st)
-            torch.cuda.synchronize()
-            if rc not in (0, None):
-                return None, None
-            if r >= 2:
-                times.append(e0.elapsed_time(e1) * 1e3)
-        res = (self.work if inplace else self.out).cpu().numpy()
-        return statistics.median(times), res
+    def restore(self):
+        for s in self.sets:
+            s.copy_(self.src)
+
+    def time(self, launch, passes):
+        """launch(ptr) sorts the batch at ptr in place; returns (us, spread, result of set 0)."""
+        us, spread = devtime.batched_us([lambda p=s.data_ptr(): launch(p) for s in self.sets], self.flush, passes,
+                                        before_pass=self.restore)
+        if us is None:
+            return None, None, None
+        return us, spread, self.sets[0].cpu().numpy()
 
 
-def run_case(dtype, n, arrays, dist, reps, results):
+def run_case(dtype, n, arrays, dist, passes, results, flags=0):
     data = workloads.make_packed(dtype, n, arrays, dist, seed=99)
     npd = bs.NP_DTYPES[dtype]
     if dtype == bs.I32:
@@ -72,31 +68,31 @@ def run_case(dtype, n, arrays, dist, reps, results):
     else:
         want = orc.sort_packed(dtype, data, n, arrays, orc.MODE_NETWORK, threads=os.cpu_count())
     timer = Timer(data)
-    st = timer.st.cuda_stream
+    st = torch.cuda.current_stream().cuda_stream
     w = working(n)
     case = {"dtype": dtype, "n": n, "arrays": arrays, "distribution": dist, "keys": n * arrays,
             "hbm_bytes": 2 * n * arrays * bs.ELEM_BYTES[dtype], "configs": []}
 
-    def record(family, cfg, us, res):
+    def record(family, cfg, timing):
+        us, spread, res = timing
         ok = None
         if res is not None:
             got = res.view(npd)
             ok = bool(np.array_equal(got["key"] if dtype else got, want["key"] if dtype else want))
-        case["configs"].append({"family": family, "config": cfg, "us": us, "ok": ok})
+        case["configs"].append({"family": family, "config": cfg, "us": us, "spread": spread, "ok": ok})
 
     for base in bs.tiles(dtype):
         tw = 1 << sum(base.as_tuple())
         if tw < n or tw > 4 * w:
             continue
-        forms = [base, base.with_persistent()]
-        if bs.tile_info(dtype, n, 0, base).tma_form:
-            forms.append(base.with_form(2))
+        info = bs.tile_info(dtype, n, 0, base)
+        forms = [base, base.with_persistent()] + ([base.with_form(2)] if info.tma_form else []) + \
+            ([base.with_form(3)] if info.xpose_form else [])
         for tile in forms:
-            us, res = timer.time(lambda i, o, t=tile: bs.sort_packed(dtype, i, o, n, arrays, 0, t, st), reps,
-                                 False)
-            record("b200sort", repr(tile), us, res)
+            record("b200sort", repr(tile),
+                   timer.time(lambda p, t=tile: bs.sort_packed_status(dtype, p, p, n, arrays, flags, t, st), passes))
 
-    if os.path.exists(CUB_LIB):
+    if os.path.exists(CUB_LIB) and not flags:
         cub = ctypes.CDLL(CUB_LIB)
         cub.cub_block_merge_sort.restype = ctypes.c_int
         cub.cub_block_merge_sort.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
@@ -104,22 +100,23 @@ def run_case(dtype, n, arrays, dist, reps, results):
         for th in (32, 64, 128, 256, 512, 1024):
             if th > w or w // th > 32:
                 continue
-            us, res = timer.time(lambda i, o, th=th: cub.cub_block_merge_sort(dtype, i, n, arrays, w, th, st),
-                                 reps, True)
-            if us is not None:
-                record("cub_block_merge", "threads=%d items=%d" % (th, w // th), us, res)
+            t = timer.time(lambda p, th=th: cub.cub_block_merge_sort(dtype, p, n, arrays, w, th, st), passes)
+            if t[0] is not None:
+                record("cub_block_merge", "threads=%d items=%d" % (th, w // th), t)
 
     if orc.ref_gpu_available() and dtype in (bs.I32, bs.I32_I32):
         suffix = "int" if dtype == bs.I32 else "rec"
         fn = getattr(orc.ref_gpu(suffix), "ref_v6_" + suffix)
+        # with B200S_SORTED_CHECK the reference runs its own Sorted switch
+        combos = ((1, 0, 0),) if flags & bs.SORTED_CHECK else ((0, 0, 0), (0, 1, 0), (0, 0, 1), (0, 1, 1))
         for th in (32, 64, 128, 256, 512, 1024):
             if th > w or w // th > 16:
                 continue
-            for sh, asy in ((0, 0), (1, 0), (0, 1), (1, 1)):
-                us, res = timer.time(lambda i, o, th=th, sh=sh, asy=asy: fn(i, n, arrays, w, th, 0, sh, asy, st),
-                                     reps, True)
-                if us is not None:
-                    record("reference_v6", "threads=%d shared=%d async=%d" % (th, sh, asy), us, res)
+            for so, sh, asy in combos:
+                t = timer.time(lambda p, th=th, so=so, sh=sh, asy=asy: fn(p, n, arrays, w, th, so, sh, asy, st),
+                               passes)
+                if t[0] is not None:
+                    record("reference_v6", "threads=%d sorted=%d shared=%d async=%d" % (th, so, sh, asy), t)
 
     best = {}
     for c in case["configs"]:
@@ -129,7 +126,7 @@ def run_case(dtype, n, arrays, dist, reps, results):
             best[c["family"]] = c
     case["best"] = best
     results.append(case)
-    line = "dtype=%d n=%d arrays=%d: " % (dtype, n, arrays) + ", ".join(
+    line = "dtype=%d n=%d arrays=%d dist=%s flags=%d: " % (dtype, n, arrays, dist, flags) + ", ".join(
         "%s %.2f us (%s)" % (f, b["us"], b["config"]) for f, b in sorted(best.items()))
     print(line, flush=True)
 
@@ -137,14 +134,21 @@ def run_case(dtype, n, arrays, dist, reps, results):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=None)
-    ap.add_argument("--reps", type=int, default=15)
+    ap.add_argument("--passes", type=int, default=5)
     ap.add_argument("--quick", action="store_true")
+    ap.add_argument("--dist", default="uniform", help="key distribution (workloads.DISTRIBUTIONS)")
+    ap.add_argument("--sorted-check", action="store_true",
+                    help="B200S_SORTED_CHECK against the reference's Sorted=true (records, n = 1000 and 2048)")
     args = ap.parse_args()
     results = []
-    run_case(bs.I32, 1024, 4096, "uniform", args.reps, results)
-    if not args.quick:
-        for n in (32, 129, 256, 1000, 2048, 4096):
-            run_case(bs.I32_I32, n, 4194304 // n, "uniform", args.reps, results)
+    if args.sorted_check:
+        for n in (1000, 2048):
+            run_case(bs.I32_I32, n, 4194304 // n, args.dist, args.passes, results, bs.SORTED_CHECK)
+    else:
+        run_case(bs.I32, 1024, 4096, args.dist, args.passes, results)
+        if not args.quick:
+            for n in (32, 129, 256, 1000, 2048, 4096):
+                run_case(bs.I32_I32, n, 4194304 // n, args.dist, args.passes, results)
     bad = [(c["n"], x["family"], x["config"]) for c in results for x in c["configs"] if x["ok"] is False]
     if args.out:
         with open(args.out, "w") as f:
