@@ -120,6 +120,9 @@ _SIGNATURES = {
     "b200s_sort_ragged_plain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                ctypes.c_void_p, ctypes.c_void_p]),
     "b200s_plan_plain_launches": (ctypes.c_int32, [ctypes.c_void_p]),
+    "b200s_sort_partitions": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    "b200s_release_partition_plans": (ctypes.c_int, []),
     "b200s_session_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32]),
     "b200s_session_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "b200s_sort_packed_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
@@ -212,6 +215,14 @@ def sort_packed(dtype, d_in, d_out, n, arrays, flags=0, tile=None, stream=0):
     tp = ctypes.byref(tile) if tile is not None else None
     return check(lib().b200s_sort_packed(dtype, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out), n, arrays,
                                          flags, tp, ctypes.c_void_p(stream)))
+
+
+def sort_partitions(dtype, d_in, d_out, d_counters, nb_parts, d_uniform=0, flags=0, stream=0):
+    """Sort every partition [counters[p], counters[p+1]) of a partitioned array
+    (the leaf of the reference's large-array sort), device pointers."""
+    return check(lib().b200s_sort_partitions(dtype, flags, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out),
+                                             ctypes.c_void_p(d_counters), ctypes.c_void_p(d_uniform or None),
+                                             nb_parts, ctypes.c_void_p(stream)))
 
 
 def sort_packed_status(dtype, d_in, d_out, n, arrays, flags=0, tile=None, stream=0):

@@ -182,6 +182,26 @@ b200s_status b200s_sort_ragged_plain(b200s_plan* plan, const void* d_in, void* d
                                      const int32_t* d_offsets, void* stream);
 int32_t b200s_plan_plain_launches(const b200s_plan* plan);
 
+/* The leaf of the reference's partitioned large-array sort: replaces the
+ * launch of SortPartitionsAdaptive_outofplace (cusort.hpp:2309-2352, launched
+ * by HybridSortPartitionedV3 at cusort.hpp:2616-2628).  Sorts every partition
+ * [d_counters[p], d_counters[p+1]) of d_in into the same range of d_out (out
+ * of place; d_in == d_out is allowed), p < nb_parts, int32 CSR counters on
+ * the device (nb_parts + 1 entries).  d_uniform (nb_parts device flags, may
+ * be NULL) marks partitions that hold a single key value, which the
+ * reference copies; sorting such a partition leaves it unchanged, so they go
+ * through the same launch.  Unlike the reference's kernel, partitions up to
+ * b200s_ragged_max_length are sorted (the reference sends those above its
+ * 48 KB rule to a separate merge sort); longer ones are not written to d_out,
+ * and the caller sorts them as the reference's merge path does.
+ * Backed by a ragged plan cached per device, element type and stream (one
+ * allocation the first time, re-captured graph when the buffers change);
+ * b200s_release_partition_plans frees the cached plans. */
+b200s_status b200s_sort_partitions(b200s_dtype dtype, uint32_t flags, const void* d_in, void* d_out,
+                                   const int32_t* d_counters, const int32_t* d_uniform, int32_t nb_parts,
+                                   void* stream);
+b200s_status b200s_release_partition_plans(void);
+
 /* No counterpart in the reference.  The ragged sort of b200s_sort_ragged for
  * callers that cannot allocate device memory: plugins inside a framework that
  * owns all device memory through its own pool, and latency-critical loops

@@ -138,6 +138,19 @@ private:
     b200s_status status_ = B200S_ERR_INVALID_ARGUMENT;
 };
 
+// The leaf of the partitioned large-array sort, under the reference kernel's
+// name (cusort.hpp:2309-2352): a host call that replaces the launch
+//   SortPartitionsAdaptive_outofplace<T, TestIfSorted, FullSM>
+//       <<<nbParts, threads, shared, stream>>>(input, output, counterParts, uniformParts, nbParts);
+// (cusort.hpp:2624-2627) with the same arguments; see b200s_sort_partitions.
+template <typename T, bool TestIfSorted = false, bool FullSM = false>
+inline b200s_status SortPartitionsAdaptive_outofplace(const T* input, T* output, const int* counterParts,
+                                                      const int* uniformParts, int nbParts,
+                                                      void* stream = nullptr) {
+    return b200s_sort_partitions(dtype_of<T>::value, TestIfSorted ? B200S_SORTED_CHECK : 0u, input, output,
+                                 counterParts, uniformParts, nbParts, stream);
+}
+
 }  // namespace b200sort
 
 #endif  // B200SORT_HPP

@@ -130,7 +130,7 @@ def ref_gpu_available():
 
 
 def ref_gpu(suffix):
-    """Reference GPU kernels ref_{v6,v3,v4,warp}_<suffix>, suffix "int" or "rec"."""
+    """Reference GPU kernels ref_{v6,v3,v4,v12,warp,partition_v3}_<suffix>, suffix "int" or "rec"."""
     global _ref_gpu
     if _ref_gpu is None:
         _ref_gpu = {}
@@ -144,5 +144,12 @@ def ref_gpu(suffix):
         fn = getattr(h, "ref_warp_%s" % suffix)
         fn.restype = ctypes.c_int
         fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        fn = getattr(h, "ref_v12_%s" % suffix)
+        fn.restype = ctypes.c_int
+        fn.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 6 + [ctypes.c_void_p]
+        fn = getattr(h, "ref_partition_v3_%s" % suffix)
+        fn.restype = ctypes.c_int
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]
         _ref_gpu[suffix] = h
     return _ref_gpu[suffix]

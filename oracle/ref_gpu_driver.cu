@@ -9,6 +9,7 @@
 //
 // REF_TYPE selects the element type of this translation unit (0 = int,
 // 1 = IntAndData); the Makefile builds one object per type.
+#include <algorithm>
 #include <cstdint>
 
 #include "cusort.hpp"
@@ -53,7 +54,28 @@ __global__ void v4_batched(Elem* data, int n, unsigned working) {
     cusort_experiment::Sort<Elem, Sorted, Shared, Async>(seg, seg, n, working);
 }
 
+// V1 / V2: one value per thread, the whole array in one block
+// (Sort_1Block_gt32_d_extsm, cusort.hpp:751-771; Sort_1Block_gt32_d_extsm_v2,
+// cusort.hpp:986-1008), launched as bench.cu:444-456 does.
+template <int Variant, bool Sorted, bool Shared>
+__global__ void v12_batched(Elem* data, int n) {
+    Elem* seg = data + size_t(blockIdx.x) * n;
+    if constexpr (Variant == 1) Sort_1Block_gt32_d_extsm<Elem, Sorted, Shared>(seg, n);
+    else Sort_1Block_gt32_d_extsm_v2<Elem, Sorted, Shared>(seg, seg, n);
+}
+
 int launch_status() { return cudaGetLastError() == cudaSuccess ? 0 : 2; }
+
+template <int Variant>
+int run_v12(Elem* d, int n, int arrays, int working, int sorted, int shared, cudaStream_t st) {
+    const size_t bytes = size_t(working) * sizeof(Elem) * (Variant == 1 ? 1 : 2);
+    const int key = (sorted ? 2 : 0) | (shared ? 1 : 0);
+    auto k = key == 0 ? v12_batched<Variant, false, false> : key == 1 ? v12_batched<Variant, false, true>
+           : key == 2 ? v12_batched<Variant, true, false> : v12_batched<Variant, true, true>;
+    if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    k<<<arrays, working, bytes, st>>>(d, n);
+    return launch_status();
+}
 
 template <unsigned W, unsigned Th, bool Sorted, bool Shared, bool Async>
 int run_v6(Elem* d, int n, int arrays, cudaStream_t st) {
@@ -155,6 +177,82 @@ int REF_SUFFIX(ref_v4)(void* d, int n, int arrays, int working, int threads, int
         case 4: v4_batched<true, false, false><<<arrays, threads, bytes, st>>>(p, n, unsigned(working)); break;
         default: return 1;
     }
+    return launch_status();
+}
+
+// Reference V1 / V2 over a packed batch, in place: working = threads, a power
+// of two in [32, 1024] and >= n.  variant 1 or 2.
+int REF_SUFFIX(ref_v12)(void* d, int n, int arrays, int variant, int working, int sorted, int shared,
+                        void* stream) {
+    if (working < 32 || working > 1024 || (working & (working - 1)) || n > working || n < 1) return 1;
+    Elem* p = static_cast<Elem*>(d);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return variant == 1 ? run_v12<1>(p, n, arrays, working, sorted, shared, st)
+                        : run_v12<2>(p, n, arrays, working, sorted, shared, st);
+}
+
+// The reference's partition stage of its large-array sort, as
+// HybridSortPartitionedV3 (cusort.hpp:2493-2588) runs it with its default
+// parameters (MaxValuesToSort 2048, MaxNbParts 1024, FullSM): pivots from the
+// data, per-partition counts and single-value flags, CSR counters, and the
+// scatter of d_data into key-range partitions.  Copies the partitioned values
+// to d_parts (n elements), the counters to d_counters (nb_parts + 1) and the
+// flags to d_uniform (nb_parts); *nb_parts_out receives the partition count
+// and *skipped_out 1 when the reference found a single partition and skipped
+// the scatter (then d_parts is d_data unchanged and there is one partition).
+int REF_SUFFIX(ref_partition_v3)(void* d_data, int n, void* d_parts, int* d_counters, int* d_uniform,
+                                 int* nb_parts_out, int* skipped_out, void* stream) {
+    constexpr int kMaxValues = 2048, kMaxParts = 1024;
+    constexpr bool kFullSM = true;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Elem* data = static_cast<Elem*>(d_data);
+    if (n <= 1) return 1;
+    CuSortWorkspace<Elem, kMaxParts> ws;
+    ws.reserve(size_t(n));
+    // the reference's step sequence (cusort.hpp:2514-2573), in its order
+    const int candidate = std::min(kMaxParts, std::max(32, 1 + (n - 1) / kMaxValues));
+    const int pivot_threads = std::max(32, GreaterPowerOf2EqualOrLarger(candidate));
+    if (pivot_threads * 2 <= DefaultNbThreadsPerBlock)
+        Sort_core_buildPivots<Elem, kMaxParts, 2, false, kFullSM><<<1, pivot_threads * 2, 0, st>>>(
+            data, n, ws.pivots(), candidate);
+    else
+        Sort_core_buildPivots<Elem, kMaxParts, 1, false, kFullSM><<<1, DefaultNbThreadsPerBlock, 0, st>>>(
+            data, n, ws.pivots(), candidate);
+    AdaptPartitionCountDevice<Elem, kMaxParts><<<1, 1, 0, st>>>(ws.pivots(), candidate, ws.activeNbParts());
+    cudaMemsetAsync(ws.counters(), 0, (candidate + 2) * sizeof(int), st);
+    const int all_blocks = (n + DefaultNbThreadsPerBlock - 1) / DefaultNbThreadsPerBlock;
+    const int blocks = std::max(1, std::min(all_blocks, ws.persistentBlocks()));
+    CountParts_Persistent<Elem, kMaxParts><<<blocks, DefaultNbThreadsPerBlock, 0, st>>>(
+        data, n, ws.pivots(), ws.blockOffsets(), ws.blockUniform(), ws.activeNbParts());
+    ReduceBlockCounts<kMaxParts, 256><<<candidate, 256, 0, st>>>(ws.blockOffsets(), ws.blockUniform(),
+                                                                 ws.counters() + 1, ws.uniformParts(), blocks,
+                                                                 ws.activeNbParts());
+    DetectSingleUniformBucket<<<1, 1, 0, st>>>(ws.counters() + 1, ws.uniformParts(), ws.activeNbParts(),
+                                               ws.skipScatterFlag());
+    BuildPrefixDynamic<int, kMaxParts><<<1, std::min(candidate, DefaultNbThreadsPerBlock), 0, st>>>(
+        ws.counters() + 1, ws.activeNbParts());
+    BuildPersistentBlockOffsets<kMaxParts><<<candidate, 1, 0, st>>>(ws.blockOffsets(), ws.counters(), blocks,
+                                                                   ws.activeNbParts());
+    MoveElements_Persistent<Elem, kMaxParts><<<blocks, DefaultNbThreadsPerBlock, 0, st>>>(
+        data, n, ws.pivots(), ws.blockOffsets(), ws.valuesBuffer(), ws.activeNbParts(), ws.skipScatterFlag());
+    int parts = 0, skipped = 0;
+    cudaMemcpyAsync(&parts, ws.activeNbParts(), sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&skipped, ws.skipScatterFlag(), sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return 2;
+    if (skipped) {
+        cudaMemcpyAsync(d_parts, data, size_t(n) * sizeof(Elem), cudaMemcpyDeviceToDevice, st);
+        const int one[2] = {0, n};
+        cudaMemcpyAsync(d_counters, one, sizeof(one), cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(d_uniform, 0xff, sizeof(int), st);
+        parts = 1;
+    } else {
+        cudaMemcpyAsync(d_parts, ws.valuesBuffer(), size_t(n) * sizeof(Elem), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(d_counters, ws.counters(), (parts + 1) * sizeof(int), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(d_uniform, ws.uniformParts(), parts * sizeof(int), cudaMemcpyDeviceToDevice, st);
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return 2;
+    *nb_parts_out = parts;
+    *skipped_out = skipped;
     return launch_status();
 }
 

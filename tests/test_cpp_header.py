@@ -22,6 +22,12 @@ int main() {
     // an empty batch is a no-op that touches no device
     bad += b200sort::Sort_1Block_v6_register<IntAndDataLike, 2048, 256, true, true, true>(nullptr, nullptr, 100, 0)
            != B200S_OK;
+    // the partition leaf under the reference kernel's name: no partitions, nothing to do;
+    // a negative count is an argument error
+    bad += b200sort::SortPartitionsAdaptive_outofplace<IntAndDataLike>(nullptr, nullptr, nullptr, nullptr, 0)
+           != B200S_OK;
+    bad += b200sort::SortPartitionsAdaptive_outofplace<int, true, true>(nullptr, nullptr, nullptr, nullptr, -1)
+           != B200S_ERR_INVALID_ARGUMENT;
     bad += b200sort::dtype_of<IntAndDataLike>::value != B200S_I32_I32;
     bad += b200sort::dtype_of<unsigned long>::value != B200S_U64;
     std::printf("%d\n", bad);

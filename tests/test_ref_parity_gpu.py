@@ -1,4 +1,4 @@
-"""GPU parity against the reference itself: its V6 / V4 / V3 / warp kernels,
+"""GPU parity against the reference itself: its V6 / V4 / V3 / V2 / V1 / warp kernels,
 compiled unmodified from its headers for sm_100a (oracle/_ref), run on the
 same inputs as the new kernels and the CPU oracle.  Records with many equal
 keys make the comparison cover the tie order, not only the keys."""
@@ -36,6 +36,8 @@ def run_ref(kind, dtype, data, n, arrays, threads=None, sorted_=0, shared=0, asy
         rc = getattr(lib, "ref_v4_" + suffix)(d.data_ptr(), n, arrays, w, threads, sorted_, shared, async_, st)
     elif kind == "v3":
         rc = getattr(lib, "ref_v3_" + suffix)(d.data_ptr(), n, arrays, w, threads, sorted_, shared, async_, st)
+    elif kind in ("v1", "v2"):
+        rc = getattr(lib, "ref_v12_" + suffix)(d.data_ptr(), n, arrays, int(kind[1]), w, sorted_, shared, st)
     else:
         rc = getattr(lib, "ref_warp_" + suffix)(d.data_ptr(), n, arrays, sorted_, shared, st)
     assert rc == 0, (kind, n, threads, rc)
@@ -105,3 +107,19 @@ def test_reference_inputs_full_batch_records():
             ref = run_ref("v6", bs.I32_I32, data, n, arrays, max(32, w // 8))
             ours = run_ours(bs.I32_I32, data, n, arrays)
             assert np.array_equal(ours, ref), (dist, n)
+
+
+@pytest.mark.parametrize("kind", ["v1", "v2"])
+@pytest.mark.parametrize("dtype", [bs.I32, bs.I32_I32])
+def test_v1_v2_equal_oracle_and_new_kernels(kind, dtype):
+    # one value per thread, the whole array in one block of `working` threads
+    # (cusort.hpp:751-771, 986-1008): every length up to 1024
+    for n in (1, 2, 17, 31, 32, 33, 100, 129, 255, 256, 500, 512, 513, 1000, 1024):
+        arrays = 5
+        for dist, extremes in INPUTS:
+            data = workloads.make_packed(dtype, n, arrays, dist, seed=n + 3, extremes=extremes)
+            oracle = orc.sort_packed(dtype, data, n, arrays, orc.MODE_NETWORK if dtype else orc.MODE_STD)
+            for sorted_, shared in ((0, 0), (1, 0), (0, 1), (1, 1)):
+                ref = run_ref(kind, dtype, data, n, arrays, sorted_=sorted_, shared=shared)
+                assert np.array_equal(ref, oracle), (kind, dtype, n, dist, sorted_, shared)
+            assert np.array_equal(run_ours(dtype, data, n, arrays), oracle), (dtype, n, dist)
