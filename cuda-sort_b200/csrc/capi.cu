@@ -287,7 +287,10 @@ b200s_status launch_packed(int idx, int persistent, const void* in, void* out, i
     const KernelEntry& e = registry()[size_t(idx)];
     if (persistent == 2 && (opts & kOptSortedCheck)) persistent = 0;
     if (persistent == 3) {
-        if (const XposeEntry* x = xpose_for(e)) {
+        const XposeEntry* x = xpose_for(e);
+        if (x && ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) % uintptr_t(x->align)) != 0)
+            x = nullptr;  // element-wide accesses need element-aligned buffers: form 0 instead
+        if (x) {
             const cudaError_t err = x->launch(in, out, n, arrays, st, opts);
             if (err != cudaSuccess) return cuda_error(err, "transposed-network sort kernel launch");
             return B200S_OK;

@@ -24,7 +24,9 @@ static void add_rec(std::vector<KernelEntry>& o) {
 void register_rec(std::vector<KernelEntry>& o) {
     add_rec<ElemRecI32>(o);
     add_rec<ElemRecI32S>(o);
-    // A warp per 1024-record array, 32 records per lane.
+    // A warp per 1024-record array, 32 records per lane; two 512-record arrays
+    // per warp (also the tile of the transposed-network form at W = 512).
+    o.push_back(Packed<ElemRecI32, 5, 4, 0>::entry(1));
     o.push_back(Packed<ElemRecI32, 5, 5, 0>::entry(1));
     o.push_back(Packed<ElemRecI32, 5, 5, 1>::entry(1));
 }

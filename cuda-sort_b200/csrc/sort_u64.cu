@@ -20,6 +20,10 @@ static void add_k16(std::vector<KernelEntry>& o) {
 
 void register_u64(std::vector<KernelEntry>& o) {
     add_k16<ElemU64, 2, 4>(o);       // W up to 8192
+    // 32 keys per lane, a warp per 1024-key array or two 512-key arrays per
+    // warp (also the tiles of the transposed-network form at those lengths)
+    o.push_back(Packed<ElemU64, 5, 4, 0>::entry(2));
+    o.push_back(Packed<ElemU64, 5, 5, 0>::entry(2));
     add_k16<ElemRecU64, 3, 3>(o);    // 16-byte registers: W up to 4096
     add_k16<ElemRecU64S, 3, 3>(o);
 }

@@ -1,7 +1,9 @@
 // Transposed-network kernels (launch form 3): every comparator layer in
 // registers, the tile re-laid out through shared memory between windows
-// (xpose.cuh).  int32 keys read and write their arrays with coalesced, striped
-// accesses (their input order is unobservable).
+// (xpose.cuh).  Keys (int32, uint64) read their arrays with coalesced striped
+// accesses (their input order is unobservable); IntAndData records load
+// coalesced through the shared region, keeping their order (the reference's
+// tie order depends on it).  Both store coalesced through the shared region.
 #include <algorithm>
 
 #include "xpose.cuh"
@@ -11,15 +13,16 @@ namespace b200s {
 
 namespace {
 
-// One warp per CTA (arrays are independent per warp, no CTA barrier), at most
-// 48 registers so that 28 warps per SM (a 4096-array batch in one wave on 148
-// SMs) are resident.
-template <class E, int LK, int LG, bool STRIPED>
+// One warp per CTA (arrays are independent per warp, no CTA barrier).  MINB
+// bounds the registers: 28 warps per SM for int32 keys (48 registers: a
+// 4096-array batch in one wave on 148 SMs); records and 64-bit keys hold twice
+// the data per element (16 warps per SM at 32 per lane, 24 at 16).
+template <class E, int LK, int LG, int IO, int MINB_ = 28>
 struct Xpose {
-    static constexpr int WPC = 1, MINB = 28;
+    static constexpr int WPC = 1, MINB = MINB_;
     static constexpr int APW = 32 >> LG;
     static constexpr size_t SMEM = size_t(WPC) * APW * xp_region<LK, LG>() * sizeof(typename E::Reg);
-    static constexpr auto kernel() { return k_sort_xpose<E, LK, LG, WPC, MINB, STRIPED>; }
+    static constexpr auto kernel() { return k_sort_xpose<E, LK, LG, WPC, MINB, IO>; }
 
     static cudaError_t launch(const void* in, void* out, int n, long long arrays, cudaStream_t st, unsigned opts) {
         const long long per_cta = (long long)WPC * APW;
@@ -32,7 +35,8 @@ struct Xpose {
         return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(kernel()));
     }
     static XposeEntry entry(int dtype) {
-        return XposeEntry{dtype, E::kStable ? 1 : 0, LK, LG, &launch, &attrs, WPC * 32, SMEM};
+        return XposeEntry{dtype, E::kStable ? 1 : 0, LK, LG, &launch, &attrs, WPC * 32, SMEM,
+                          int(sizeof(typename E::Mem))};
     }
 };
 
@@ -42,9 +46,25 @@ const std::vector<XposeEntry>& xpose_registry() {
     static const std::vector<XposeEntry> all = [] {
         std::vector<XposeEntry> v;
         constexpr int I32 = 0;                              // B200S_I32
-        v.push_back(Xpose<ElemI32, 5, 5, true>::entry(I32));  // W = 1024, a warp per array
-        v.push_back(Xpose<ElemI32, 5, 4, true>::entry(I32));  // W = 512, two arrays per warp
-        v.push_back(Xpose<ElemI32, 5, 3, true>::entry(I32));  // W = 256, four arrays per warp
+        v.push_back(Xpose<ElemI32, 5, 5, kXpIoStriped>::entry(I32));  // W = 1024, a warp per array
+        v.push_back(Xpose<ElemI32, 5, 4, kXpIoStriped>::entry(I32));  // W = 512, two arrays per warp
+        v.push_back(Xpose<ElemI32, 5, 3, kXpIoStriped>::entry(I32));  // W = 256, four arrays per warp
+        constexpr int REC = 1;                                     // B200S_I32_I32, reference tie order
+        v.push_back(Xpose<ElemRecI32, 5, 5, kXpIoStaged, 16>::entry(REC));  // W = 1024
+        v.push_back(Xpose<ElemRecI32, 5, 4, kXpIoStaged, 16>::entry(REC));  // W = 512
+        v.push_back(Xpose<ElemRecI32, 4, 4, kXpIoStaged, 24>::entry(REC));  // W = 256
+        v.push_back(Xpose<ElemRecI32, 4, 3, kXpIoStaged, 24>::entry(REC));  // W = 128
+        v.push_back(Xpose<ElemRecI32, 4, 2, kXpIoStaged, 24>::entry(REC));  // W = 64
+        // stable records: (key, data, position) registers, 16 per lane
+        v.push_back(Xpose<ElemRecI32S, 4, 4, kXpIoStaged, 20>::entry(REC));  // W = 256
+        v.push_back(Xpose<ElemRecI32S, 4, 3, kXpIoStaged, 20>::entry(REC));  // W = 128
+        v.push_back(Xpose<ElemRecI32S, 4, 2, kXpIoStaged, 20>::entry(REC));  // W = 64
+        constexpr int U64 = 2;                                     // B200S_U64
+        v.push_back(Xpose<ElemU64, 5, 5, kXpIoStriped, 16>::entry(U64));    // W = 1024
+        v.push_back(Xpose<ElemU64, 5, 4, kXpIoStriped, 16>::entry(U64));    // W = 512
+        v.push_back(Xpose<ElemU64, 4, 4, kXpIoStriped, 24>::entry(U64));    // W = 256
+        v.push_back(Xpose<ElemU64, 4, 3, kXpIoStriped, 24>::entry(U64));    // W = 128
+        v.push_back(Xpose<ElemU64, 4, 2, kXpIoStriped, 24>::entry(U64));    // W = 64
         return v;
     }();
     return all;

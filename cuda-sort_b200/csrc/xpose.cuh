@@ -68,6 +68,23 @@ __device__ __forceinline__ void xcex(typename E::Reg& lo, typename E::Reg& hi) {
     else E::cex(lo, hi);
 }
 
+// Streaming (evict-first) global accesses of one element of each memory
+// layout; records move as one 8- or 16-byte access, so their arrays must be
+// aligned to the record size (the C ABI checks before choosing this form).
+__device__ __forceinline__ int32_t xp_ldcs(const int32_t* p) { return __ldcs(p); }
+__device__ __forceinline__ uint64_t xp_ldcs(const uint64_t* p) {
+    return __ldcs(reinterpret_cast<const unsigned long long*>(p));
+}
+__device__ __forceinline__ RecI32 xp_ldcs(const RecI32* p) {
+    const int2 v = __ldcs(reinterpret_cast<const int2*>(p));
+    return RecI32{v.x, v.y};
+}
+__device__ __forceinline__ void xp_stcs(int32_t* p, int32_t v) { __stcs(p, v); }
+__device__ __forceinline__ void xp_stcs(uint64_t* p, uint64_t v) {
+    __stcs(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
+}
+__device__ __forceinline__ void xp_stcs(RecI32* p, RecI32 v) { __stcs(reinterpret_cast<int2*>(p), make_int2(v.key, v.data)); }
+
 template <int LK>
 __host__ __device__ constexpr int xp_addr(int i) {
     return i + (i >> LK);
@@ -208,14 +225,42 @@ __device__ __forceinline__ void xp_load_striped(typename E::Reg (&v)[1 << LK], c
     constexpr int K = 1 << LK, G = 1 << LG;
     if (n == K * G) {
 #pragma unroll
-        for (int q = 0; q < K; ++q) v[q] = E::from_mem(__ldcs(src + q * G + t), q * G + t);
+        for (int q = 0; q < K; ++q) v[q] = E::from_mem(xp_ldcs(src + q * G + t), q * G + t);
     } else {
 #pragma unroll
         for (int q = 0; q < K; ++q) {
             const int idx = q * G + t;
-            v[q] = idx < n ? E::from_mem(__ldcs(src + idx), idx) : E::pad();
+            v[q] = idx < n ? E::from_mem(xp_ldcs(src + idx), idx) : E::pad();
         }
     }
+}
+
+// Coalesced load that keeps the input order (any element type): lane t reads
+// elements t, t + G, ... (for 8-byte records one 256-byte row per warp
+// instruction), writes each at its logical address in the shared region, and
+// reads its natural-layout registers [t*K, t*K + K) back; conflict-free like
+// the store below.  Elements at or beyond n are padding.
+template <class E, int LK, int LG>
+__device__ __forceinline__ void xp_load_staged(typename E::Reg (&v)[1 << LK], const typename E::Mem* src,
+                                               const int t, const int n, typename E::Reg* sm) {
+    constexpr int K = 1 << LK, G = 1 << LG;
+    if (n == K * G) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) sm[xp_addr<LK>(q * G + t)] = E::from_mem(xp_ldcs(src + q * G + t), q * G + t);
+    } else {
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const int idx = q * G + t;
+            sm[xp_addr<LK>(idx)] = idx < n ? E::from_mem(xp_ldcs(src + idx), idx) : E::pad();
+        }
+    }
+    __syncwarp();
+    const int bn = xp_addr<LK>(t << LK);
+    sfor<0, K>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        v[q] = sm[bn + xp_addr<LK>(q)];
+    });
+    __syncwarp();
 }
 
 // Store the sorted natural-layout tile (lane t holds [t*K, t*K + K)) through
@@ -235,28 +280,33 @@ __device__ __forceinline__ void xp_store_striped(typename E::Reg (&v)[1 << LK], 
     __syncwarp();
     if (n == K * G) {
 #pragma unroll
-        for (int q = 0; q < K; ++q) __stcs(dst + q * G + t, E::to_mem(sm[xp_addr<LK>(q * G + t)]));
+        for (int q = 0; q < K; ++q) xp_stcs(dst + q * G + t, E::to_mem(sm[xp_addr<LK>(q * G + t)]));
     } else {
 #pragma unroll
         for (int q = 0; q < K; ++q) {
             const int idx = q * G + t;
             const typename E::Reg x = sm[xp_addr<LK>(idx)];
-            if (idx < n) __stcs(dst + idx, E::to_mem(x));
+            if (idx < n) xp_stcs(dst + idx, E::to_mem(x));
         }
     }
     __syncwarp();
 }
 
 // Packed batch (array a at [a*n, a*n + n)): each warp sorts 32/G arrays at a
-// time and strides over the batch by the whole grid.  STRIPED (keys alone):
-// coalesced loads and stores as above; otherwise each lane moves its K
-// consecutive elements with 128-bit accesses.  PF: the warp loads its next
+// time and strides over the batch by the whole grid.  IO selects how arrays
+// move: kXpIoBlocked, each lane its K consecutive elements with 128-bit
+// accesses; kXpIoStriped (keys alone), coalesced relabelling loads; kXpIoStaged
+// (any element type), coalesced loads through the shared region.  Both
+// coalesced forms store through the shared region, coalesced.  PF: the warp loads its next
 // arrays into registers before sorting the current ones, so that with a grid
 // of a few warps per SM the loads of one round overlap the sorting of the
 // previous one.  No CTA-wide barrier: every warp runs on its own.
-template <class E, int LK, int LG, int WPC, int MINB, bool STRIPED, bool PF = false>
+constexpr int kXpIoBlocked = 0, kXpIoStriped = 1, kXpIoStaged = 2;
+
+template <class E, int LK, int LG, int WPC, int MINB, int IO, bool PF = false>
 __global__ void __launch_bounds__(WPC * 32, MINB)
     k_sort_xpose(const typename E::Mem* in, typename E::Mem* out, int n, long long arrays, unsigned opts) {
+    constexpr bool STRIPED = IO == kXpIoStriped;
     using R = typename E::Reg;
     constexpr int K = 1 << LK, G = 1 << LG, APW = 32 / G;
     static_assert(LG <= 5 && LG <= LK && LG >= 1, "one warp or less per array, at most two windows");
@@ -273,8 +323,12 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
     auto load = [&](R (&x)[K], long long a) {
         const int na = a < arrays ? n : 0;
         const typename E::Mem* src = in + (a < arrays ? a : 0) * (long long)n;
-        if (STRIPED && !check) xp_load_striped<E, LK, LG>(x, src, t, na);
-        else load_tile<E, K>(x, src, t * K, na);
+        if constexpr (IO == kXpIoStaged) {
+            xp_load_staged<E, LK, LG>(x, src, t, na, sm);
+        } else {
+            if (STRIPED && !check) xp_load_striped<E, LK, LG>(x, src, t, na);
+            else load_tile<E, K>(x, src, t * K, na);
+        }
     };
     auto finish = [&](R (&x)[K], long long a) {
         bool skip = false;
@@ -283,7 +337,7 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
         if (skip && in == out) return;  // in order and in place: nothing to write
         const int na = a < arrays ? n : 0;
         typename E::Mem* dst = out + (a < arrays ? a : 0) * (long long)n;
-        if constexpr (STRIPED) xp_store_striped<E, LK, LG>(x, dst, t, na, sm);
+        if constexpr (IO != kXpIoBlocked) xp_store_striped<E, LK, LG>(x, dst, t, na, sm);
         else store_tile<E, K>(x, dst, t * K, na);
     };
     R v[K];

@@ -16,6 +16,7 @@ struct XposeEntry {
     cudaError_t (*attrs)(cudaFuncAttributes* attr);
     int cta;      // threads per CTA
     size_t smem;  // dynamic shared memory per CTA
+    int align;    // the arrays' buffers must be aligned to this many bytes (one element)
 };
 
 const std::vector<XposeEntry>& xpose_registry();
