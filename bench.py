@@ -550,6 +550,48 @@ def gpu_baselines(ctx, wl, data, host, ours_tile):
     return out
 
 
+def bucket_breakdown(ctx, wl, data, off):
+    """Per power-of-two length class: the persistent graph form on a batch
+    holding only that class's arrays of the same input (device time, median
+    of 5 batched passes), its arrays and elements, and its share of the sum."""
+    torch = ctx.torch
+    dtype, flags = wl["dtype"], wl["flags"]
+    lens = np.diff(off)
+    cls = np.where(lens > 0, np.ceil(np.log2(np.maximum(lens, 1))).astype(np.int64), -1)
+    rows = []
+    for L in sorted(set(cls[cls >= 0].tolist())):
+        ids = np.nonzero(cls == L)[0]
+        sub_len = lens[ids]
+        sub_off = np.zeros(len(ids) + 1, dtype=np.int64)
+        np.cumsum(sub_len, out=sub_off[1:])
+        idx = np.concatenate([np.arange(off[a], off[a + 1]) for a in ids])
+        sub = data[idx]
+        d_in = torch.from_numpy(sub.view(np.uint8).copy()).to(ctx.dev)
+        d_out = torch.empty_like(d_in)
+        d_off = torch.from_numpy(sub_off.astype(np.int32)).to(ctx.dev)
+        with bs.Plan(dtype, len(ids), flags, ctx.local) as plan:
+            def step(i):
+                plan.sort(d_in.data_ptr(), d_out.data_ptr(), d_off.data_ptr(), len(ids), ctx.sh)
+            step(0)
+            times = [ctx.event_time(step, 5) / 5 for _ in range(5)]
+            # the same class through the plain form (one launch of the tabled tile of W)
+            plan.prepare_plain(sub_off.astype(np.int32), by_bucket=True)
+
+            def plain(i):
+                plan.sort_plain(d_in.data_ptr(), d_out.data_ptr(), d_off.data_ptr(), ctx.sh)
+            plain(0)
+            ptimes = [ctx.event_time(plain, 5) / 5 for _ in range(5)]
+        rows.append({"working_length": 1 << L, "arrays": int(len(ids)), "elements": int(sub_len.sum()),
+                     "ms": statistics.median(times), "plain_ms": statistics.median(ptimes)})
+    total = sum(r["ms"] for r in rows)
+    for r in rows:
+        r["share"] = r["ms"] / total if total else 0.0
+    return {"method": "each length class alone through its own plan (graph replay) and through the plain form "
+                      "(one launch of the tabled tile), 5 back-to-back steps between CUDA events, median of 5; "
+                      "shares of the sum of the classes", "classes": rows, "sum_ms": total,
+            "plain_sum_ms": sum(r["plain_ms"] for r in rows)}
+
+
 def verify_ragged(dtype, data, off, got):
     """Size-independent checks: sorted within every array, per-array key sums
     equal, and (records) every payload is the position of an equal key of the
@@ -644,10 +686,21 @@ def run_gpu(args, wl):
         psteps = max(2, min(args.steps, 5))
         ms_plain = ctx.event_time(plain, psteps) / psteps
         verified = verified and verify_ragged(dtype, data, off, d_out.cpu().numpy().view(bs.NP_DTYPES[dtype]))
-        extra["baselines"] = {"plain_per_length": {
-            "ms_per_step": ms_plain, "value": total_keys * ctx.world / (ms_plain * 1e-3), "unit": UNIT,
-            "launches_per_step": plain_launches,
-            "persistent_graph_speedup": ms_plain / ms_step}}
+        # the same kernels launched once per power-of-two length class
+        bucket_launches = plan.prepare_plain(off.astype(np.int32), by_bucket=True)
+        for i in range(2):
+            plain(i)
+        ms_bucket = ctx.event_time(plain, psteps) / psteps
+        verified = verified and verify_ragged(dtype, data, off, d_out.cpu().numpy().view(bs.NP_DTYPES[dtype]))
+        extra["baselines"] = {
+            "plain_per_length": {
+                "ms_per_step": ms_plain, "value": total_keys * ctx.world / (ms_plain * 1e-3), "unit": UNIT,
+                "launches_per_step": plain_launches, "persistent_graph_speedup": ms_plain / ms_step},
+            "plain_per_bucket": {
+                "ms_per_step": ms_bucket, "value": total_keys * ctx.world / (ms_bucket * 1e-3), "unit": UNIT,
+                "launches_per_step": bucket_launches, "persistent_graph_speedup": ms_bucket / ms_step}}
+        if ctx.world == 1:
+            extra["bucket_breakdown"] = bucket_breakdown(ctx, wl, data, off)
 
     value = weak_value(total_keys, ctx.world, ms_step)
     hbm, peak_src = peaks()

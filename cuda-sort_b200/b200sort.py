@@ -120,6 +120,7 @@ _SIGNATURES = {
     "b200s_sort_ragged_plain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                ctypes.c_void_p, ctypes.c_void_p]),
     "b200s_plan_plain_launches": (ctypes.c_int32, [ctypes.c_void_p]),
+    "b200s_plan_prepare_plain_buckets": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]),
     "b200s_sort_partitions": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     "b200s_release_partition_plans": (ctypes.c_int, []),
@@ -282,9 +283,12 @@ class Plan:
         check(lib().b200s_plan_too_long(self._h, ctypes.c_void_p(stream), ctypes.byref(c)))
         return c.value
 
-    def prepare_plain(self, h_offsets_int32):
+    def prepare_plain(self, h_offsets_int32, by_bucket=False):
+        """Group the arrays for the plain form: by exact length, or by_bucket by
+        power-of-two working length; returns the launches per sort."""
         off = np.ascontiguousarray(h_offsets_int32, dtype=np.int32)
-        check(lib().b200s_plan_prepare_plain(self._h, ctypes.c_void_p(off.ctypes.data), len(off) - 1))
+        fn = lib().b200s_plan_prepare_plain_buckets if by_bucket else lib().b200s_plan_prepare_plain
+        check(fn(self._h, ctypes.c_void_p(off.ctypes.data), len(off) - 1))
         return lib().b200s_plan_plain_launches(self._h)
 
     def sort_plain(self, d_in, d_out, d_offsets, stream=0):

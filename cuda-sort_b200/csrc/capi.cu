@@ -198,7 +198,7 @@ b200s_status parse_table_file(const char* path, TableRows* out) {
         if (line[first] == 'r') {
             std::string tag;
             int d, fl, w, fam;
-            if (!(ss >> tag >> d >> fl >> w >> fam) || !valid_dtype(d) || w < 3 || w > 18 || fam < 0 || fam > 1)
+            if (!(ss >> tag >> d >> fl >> w >> fam) || !valid_dtype(d) || w < 3 || w > 18 || fam < 0 || fam > 2)
                 return set_error(B200S_ERR_INVALID_ARGUMENT,
                                  "tile table line " + std::to_string(lineno) + ": bad ragged row");
             out->ragged.push_back({d, effective_stable(d, uint32_t(fl)), w, fam});

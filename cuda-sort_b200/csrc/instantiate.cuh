@@ -22,7 +22,9 @@ struct Packed {
     // record per kernel of this tile (0 packed, 1 list, 2 persistent).
     template <int WHICH>
     static cudaError_t prepare(const void* fn) {
-        if (SMEM <= 48 * 1024) return cudaSuccess;
+        // the default limit covers static + dynamic shared memory: opt in
+        // with a margin for the kernels' own static variables
+        if (SMEM + 1024 <= 48 * 1024) return cudaSuccess;
         static std::atomic<unsigned long long> done{0};
         int dev = 0;
         cudaError_t e = cudaGetDevice(&dev);
@@ -49,7 +51,36 @@ struct Packed {
         if (e != cudaSuccess) return e;
         const int grid = (count + CTA / S::TPA - 1) / (CTA / S::TPA);
         fn<<<dim3(unsigned(grid)), dim3(CTA), SMEM, st>>>(
-            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), off, ids, count);
+            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), off, ids, count, nullptr,
+            nullptr, nullptr);
+        return cudaGetLastError();
+    }
+    // Over a dedicated bucket of a ragged plan: count and list position read
+    // on the device; the grid is the resident capacity (cached per device),
+    // at most what max_count arrays need, pulling arrays from the queue at
+    // d_head (zero before the launch).
+    static cudaError_t launch_list_dev(const void* in, void* out, const int* off, const int* ids, const int* d_count,
+                                       const int* d_base, int* d_head, int max_count, cudaStream_t st) {
+        auto fn = k_sort_idlist<E, S, CTA, SB>;
+        cudaError_t e = prepare<1>(reinterpret_cast<const void*>(fn));
+        if (e != cudaSuccess) return e;
+        static std::atomic<int> resident[64];
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        int cap = resident[dev & 63].load(std::memory_order_relaxed);
+        if (cap == 0) {
+            int per_sm = 0, sms = 0;
+            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, CTA, SMEM)) != cudaSuccess) return e;
+            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+            cap = per_sm * sms;
+            if (cap <= 0) return cudaErrorInvalidConfiguration;
+            resident[dev & 63].store(cap, std::memory_order_relaxed);
+        }
+        const int need = (max_count + CTA / S::TPA - 1) / (CTA / S::TPA);
+        const int grid = need < cap ? (need > 0 ? need : 1) : cap;
+        fn<<<dim3(unsigned(grid)), dim3(CTA), SMEM, st>>>(static_cast<const typename E::Mem*>(in),
+                                                          static_cast<typename E::Mem*>(out), off, ids, 0, d_count,
+                                                          d_base, d_head);
         return cudaGetLastError();
     }
     // Persistent launch: as many CTAs as fit at once (cached per device), never
@@ -85,7 +116,7 @@ struct Packed {
     static KernelEntry entry(int dtype) {
         return KernelEntry{dtype,   E::kStable ? 1 : 0, LK,     LG,         LW,
                            CTA,     S::LOGW,            SMEM,   CTA / S::TPA, &launch,
-                           &attrs,  &launch_list,       &launch_pf, -1,   nullptr};
+                           &attrs,  &launch_list,       &launch_pf, -1,   nullptr, &launch_list_dev};
     }
 };
 
@@ -162,7 +193,7 @@ struct ClusterTile {
     }
     static KernelEntry entry(int dtype) {
         return KernelEntry{dtype, E::kStable ? 1 : 0, LK, LG, LW, CTA, S::LOGW + LC, SMEM, 1, &launch, &attrs,
-                           &launch_list, &launch, LC, &launch_cluster_list};
+                           &launch_list, &launch, LC, &launch_cluster_list, nullptr};
     }
 };
 
@@ -171,7 +202,7 @@ template <class E, int CTA, int NB, int LKA, int LKB, bool SB = false, int MINB 
 struct Ragged {
     static constexpr size_t SMEM = ragged_smem<E, CTA, NB, LKA, LKB, SB>();
     static cudaError_t launch(const void* in, void* out, const int* off, const int* ids, RaggedCtl* ctl,
-                              unsigned family_mask, int grid, cudaStream_t st) {
+                              unsigned family_mask, unsigned dedicated_mask, int grid, cudaStream_t st) {
         auto fn = k_sort_ragged<E, CTA, NB, LKA, LKB, SB, MINB>;
         if (SMEM > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
@@ -180,7 +211,7 @@ struct Ragged {
         }
         fn<<<dim3(unsigned(grid)), dim3(CTA), SMEM, st>>>(static_cast<const typename E::Mem*>(in),
                                                           static_cast<typename E::Mem*>(out), off, ids, ctl,
-                                                          family_mask);
+                                                          family_mask, dedicated_mask);
         return cudaGetLastError();
     }
     static int resident_per_sm() {

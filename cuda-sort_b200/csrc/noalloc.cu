@@ -31,6 +31,9 @@ b200s_status set_error(b200s_status s, const std::string& msg);
 b200s_status cuda_error(cudaError_t e, const char* what);
 int effective_stable(int dtype, uint32_t flags);
 unsigned ragged_family_mask(int dtype, int stable);
+unsigned ragged_dedicated_mask(int dtype, int stable);
+void dedicated_entries(int dtype, int stable, int nb, unsigned* mask, int* idx);
+int lookup_default_entry(int dtype, int stable, long long n, int* persistent);
 
 namespace {
 
@@ -126,8 +129,26 @@ extern "C" b200s_status b200s_sort_ragged_noalloc(b200s_dtype dtype, uint32_t fl
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "bin count launch");
     k_bin_scatter<<<bin_grid, bin_threads, 0, cs>>>(d_offsets, n, &s->ctl, s->ids, s->oids, spec);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "bin scatter launch");
-    e = rk->launch(d_in, d_out, d_offsets, s->ids, &s->ctl, ragged_family_mask(dtype, stable), sms * per_sm, cs);
-    if (e != cudaSuccess) return cuda_error(e, "ragged sort launch");
+    // the plan's routing: buckets with their own launch run after the
+    // persistent kernel on the same stream (no side streams here); the tile
+    // table that sets it loads on the first lookup
+    int unused_form = 0;
+    (void)lookup_default_entry(dtype, stable, 1, &unused_form);
+    unsigned dedicated = ragged_dedicated_mask(dtype, stable);
+    int dedicated_idx[kMaxBuckets] = {};
+    dedicated_entries(dtype, stable, rk->nb, &dedicated, dedicated_idx);
+    if (dedicated != (1u << rk->nb) - 1u) {
+        e = rk->launch(d_in, d_out, d_offsets, s->ids, &s->ctl, ragged_family_mask(dtype, stable), dedicated,
+                       sms * per_sm, cs);
+        if (e != cudaSuccess) return cuda_error(e, "ragged sort launch");
+    }
+    for (int b = rk->nb - 1; b >= 0; --b) {
+        if (!((dedicated >> b) & 1u)) continue;
+        const KernelEntry& k = registry()[size_t(dedicated_idx[b])];
+        e = k.launch_list_dev(d_in, d_out, d_offsets, s->ids, &s->ctl.count[b], &s->ctl.base[b], &s->ctl.dhead[b], n,
+                              cs);
+        if (e != cudaSuccess) return cuda_error(e, "dedicated bucket launch");
+    }
     for (int i = 0; i < spec.n_over; ++i) {
         const KernelEntry& k = registry()[size_t(cluster_idx[i])];
         e = k.launch_cluster_list(d_in, d_out, d_offsets, s->oids + size_t(i) * kNoAllocArrays, &s->ctl.ocount[i],

@@ -37,6 +37,7 @@ namespace {
 
 std::mutex g_mask_mutex;
 unsigned g_family_mask[4][2] = {};
+unsigned g_dedicated_mask[4][2] = {};
 
 const RaggedEntry* find_ragged(int dtype, int stable) {
     for (const RaggedEntry& e : ragged_registry())
@@ -46,17 +47,45 @@ const RaggedEntry* find_ragged(int dtype, int stable) {
 
 }  // namespace
 
+// Ragged table rows: family 0 (A) or 1 (B) runs the bucket in the persistent
+// kernel with that shape family; family 2 gives the bucket its own launch of
+// the packed tile the tile table chooses for its working length.
 void set_ragged_family(int dtype, int stable, int log2w, int family) {
     std::lock_guard<std::mutex> lock(g_mask_mutex);
     const int b = log2w - kRaggedLmin;
     if (b < 0 || b >= kMaxBuckets) return;
-    if (family) g_family_mask[dtype][stable] |= 1u << b;
+    if (family == 1) g_family_mask[dtype][stable] |= 1u << b;
     else g_family_mask[dtype][stable] &= ~(1u << b);
+    if (family == 2) g_dedicated_mask[dtype][stable] |= 1u << b;
+    else g_dedicated_mask[dtype][stable] &= ~(1u << b);
 }
 
 unsigned ragged_family_mask(int dtype, int stable) {
     std::lock_guard<std::mutex> lock(g_mask_mutex);
     return g_family_mask[dtype][stable];
+}
+
+unsigned ragged_dedicated_mask(int dtype, int stable) {
+    std::lock_guard<std::mutex> lock(g_mask_mutex);
+    return g_dedicated_mask[dtype][stable];
+}
+
+// Registry entries of the dedicated buckets (bit b of `mask`: bucket b, W =
+// 2^(kRaggedLmin + b)): the tabled single-CTA tile of that working length.
+// Buckets without one (none tabled, or a cluster tile) stay in the persistent
+// kernel: their bit is cleared in *mask.  idx[b] receives the entry.
+void dedicated_entries(int dtype, int stable, int nb, unsigned* mask, int* idx) {
+    for (int b = 0; b < nb; ++b) {
+        idx[b] = -1;
+        if (!((*mask >> b) & 1u)) continue;
+        int persistent = 0;
+        const int e = lookup_default_entry(dtype, stable, 1LL << (kRaggedLmin + b), &persistent);
+        if (e >= 0 && registry()[size_t(e)].lc < 0 && registry()[size_t(e)].launch_list_dev &&
+            registry()[size_t(e)].log2w == kRaggedLmin + b)
+            idx[b] = e;
+        else
+            *mask &= ~(1u << b);
+    }
 }
 
 }  // namespace b200s
@@ -71,6 +100,8 @@ struct b200s_plan {
     long long max_arrays = 0;
     const RaggedEntry* rk = nullptr;
     unsigned family_mask = 0;
+    unsigned dedicated_mask = 0;         // buckets with their own launch
+    int dedicated_entry[kMaxBuckets] = {};
     int grid = 0;       // persistent CTAs
     int bin_grid = 0;   // CTAs of the binning kernels
     void* scratch = nullptr;
@@ -79,9 +110,10 @@ struct b200s_plan {
     int* oids = nullptr;          // cluster-bucket id lists, stride max_arrays
     BinSpec spec = {};
     int over_entry[kMaxOverflow] = {};  // registry index of each cluster bucket
+    static constexpr int kSides = 4;
     cudaStream_t capture = nullptr;
-    cudaStream_t side = nullptr;  // cluster buckets run beside the persistent kernel
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t side[kSides] = {};  // cluster and dedicated buckets run beside the persistent kernel
+    cudaEvent_t fork = nullptr, join[kSides] = {};
     // the graph of the last (in, out, offsets, arrays)
     cudaGraphExec_t exec = nullptr;
     const void* g_in = nullptr;
@@ -108,23 +140,46 @@ b200s_status record_sequence(b200s_plan* p, const void* in, void* out, const int
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "bin count launch");
     k_bin_scatter<<<bin_grid, bin_threads, 0, st>>>(off, arrays, p->ctl, p->ids, p->oids, p->spec);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "bin scatter launch");
-    if (p->spec.n_over > 0) {
-        // Fork: the cluster buckets run on the side stream while the
-        // persistent kernel runs on st; join before returning.
-        if ((e = cudaEventRecord(p->fork, st)) != cudaSuccess) return cuda_error(e, "fork record");
-        if ((e = cudaStreamWaitEvent(p->side, p->fork, 0)) != cudaSuccess) return cuda_error(e, "fork wait");
-        for (int i = 0; i < p->spec.n_over; ++i) {
-            const KernelEntry& k = registry()[size_t(p->over_entry[i])];
-            e = k.launch_cluster_list(in, out, off, p->oids + size_t(i) * p->spec.stride, &p->ctl->ocount[i],
-                                      int(std::min<long long>(arrays, p->max_arrays)), p->side);
-            if (e != cudaSuccess) return cuda_error(e, "cluster bucket launch");
+    // Fork: the cluster buckets and the dedicated buckets run on side streams
+    // (largest first, round robin) while the persistent kernel runs on st;
+    // join before returning.
+    const int max_count = int(std::min<long long>(arrays, p->max_arrays));
+    int used = 0;
+    auto side_stream = [&](int k) -> cudaStream_t {
+        const int s = k % b200s_plan::kSides;
+        if (s >= used) {
+            if (used == 0 && (e = cudaEventRecord(p->fork, st)) != cudaSuccess) return nullptr;
+            if ((e = cudaStreamWaitEvent(p->side[s], p->fork, 0)) != cudaSuccess) return nullptr;
+            used = s + 1;
         }
-        if ((e = cudaEventRecord(p->join, p->side)) != cudaSuccess) return cuda_error(e, "join record");
+        return p->side[s];
+    };
+    int k = 0;
+    for (int i = p->spec.n_over - 1; i >= 0; --i, ++k) {
+        const KernelEntry& ke = registry()[size_t(p->over_entry[i])];
+        cudaStream_t ss = side_stream(k);
+        if (!ss) return cuda_error(e, "fork");
+        e = ke.launch_cluster_list(in, out, off, p->oids + size_t(i) * p->spec.stride, &p->ctl->ocount[i],
+                                   max_count, ss);
+        if (e != cudaSuccess) return cuda_error(e, "cluster bucket launch");
     }
-    e = p->rk->launch(in, out, off, p->ids, p->ctl, p->family_mask, p->grid, st);
-    if (e != cudaSuccess) return cuda_error(e, "ragged sort launch");
-    if (p->spec.n_over > 0 && (e = cudaStreamWaitEvent(st, p->join, 0)) != cudaSuccess)
-        return cuda_error(e, "join wait");
+    for (int b = p->spec.nb - 1; b >= 0; --b) {
+        if (!((p->dedicated_mask >> b) & 1u)) continue;
+        const KernelEntry& ke = registry()[size_t(p->dedicated_entry[b])];
+        cudaStream_t ss = side_stream(k++);
+        if (!ss) return cuda_error(e, "fork");
+        e = ke.launch_list_dev(in, out, off, p->ids, &p->ctl->count[b], &p->ctl->base[b], &p->ctl->dhead[b],
+                               max_count, ss);
+        if (e != cudaSuccess) return cuda_error(e, "dedicated bucket launch");
+    }
+    if (p->dedicated_mask != (1u << p->spec.nb) - 1u) {
+        e = p->rk->launch(in, out, off, p->ids, p->ctl, p->family_mask, p->dedicated_mask, p->grid, st);
+        if (e != cudaSuccess) return cuda_error(e, "ragged sort launch");
+    }
+    for (int s = 0; s < used; ++s) {
+        if ((e = cudaEventRecord(p->join[s], p->side[s])) != cudaSuccess) return cuda_error(e, "join record");
+        if ((e = cudaStreamWaitEvent(st, p->join[s], 0)) != cudaSuccess) return cuda_error(e, "join wait");
+    }
     return B200S_OK;
 }
 
@@ -191,7 +246,13 @@ b200s_status b200s_plan_create(b200s_plan** out, b200s_dtype dtype, uint32_t fla
     p->flags = flags;
     p->max_arrays = max_arrays;
     p->rk = rk;
+    // The tile table (its packed rows and the ragged rows that set the masks
+    // below) loads on the first lookup: make sure it has.
+    int unused_form = 0;
+    (void)lookup_default_entry(dtype, stable, 1, &unused_form);
     p->family_mask = ragged_family_mask(dtype, stable);
+    p->dedicated_mask = ragged_dedicated_mask(dtype, stable);
+    dedicated_entries(dtype, stable, rk->nb, &p->dedicated_mask, p->dedicated_entry);
     p->grid = sms * per_sm;
     p->bin_grid = sms * 4;
     const long long stride = std::max<long long>(1, max_arrays);
@@ -210,10 +271,13 @@ b200s_status b200s_plan_create(b200s_plan** out, b200s_dtype dtype, uint32_t fla
     p->ids = reinterpret_cast<int*>(static_cast<char*>(p->scratch) + sizeof(RaggedCtl));
     p->plain_ids = p->ids + stride;
     p->oids = p->plain_ids + stride;
-    if ((e = cudaStreamCreateWithFlags(&p->capture, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming)) != cudaSuccess) {
+    e = cudaStreamCreateWithFlags(&p->capture, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming);
+    for (int s = 0; s < b200s_plan::kSides && e == cudaSuccess; ++s) {
+        e = cudaStreamCreateWithFlags(&p->side[s], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->join[s], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
         b200s_plan_destroy(p);
         return cuda_error(e, "plan streams");
     }
@@ -228,9 +292,11 @@ b200s_status b200s_plan_destroy(b200s_plan* p) {
     cudaDeviceSynchronize();
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->capture) cudaStreamDestroy(p->capture);
-    if (p->side) cudaStreamDestroy(p->side);
+    for (int s = 0; s < b200s_plan::kSides; ++s) {
+        if (p->side[s]) cudaStreamDestroy(p->side[s]);
+        if (p->join[s]) cudaEventDestroy(p->join[s]);
+    }
     if (p->fork) cudaEventDestroy(p->fork);
-    if (p->join) cudaEventDestroy(p->join);
     if (p->scratch) cudaFree(p->scratch);
     delete p;
     return B200S_OK;
@@ -293,37 +359,66 @@ b200s_status b200s_plan_too_long(b200s_plan* p, void* stream, int64_t* count) {
     return B200S_OK;
 }
 
-b200s_status b200s_plan_prepare_plain(b200s_plan* p, const int32_t* h_offsets, int64_t arrays) {
+}  // extern "C"
+
+namespace {
+
+// Groups the arrays on the host, uploads the id lists and records one launch
+// per group: by exact length (by_bucket false: every array of a group has the
+// same length) or by power-of-two working length (by_bucket true: the tile of
+// W = 2^L sorts every array of length (W/2, W]; each array's own length comes
+// from the offsets).
+b200s_status prepare_plain(b200s_plan* p, const int32_t* h_offsets, int64_t arrays, bool by_bucket) {
     if (!p || (!h_offsets && arrays > 0)) return set_error(B200S_ERR_INVALID_ARGUMENT, "null argument");
     if (arrays < 0 || arrays > p->max_arrays)
         return set_error(B200S_ERR_INVALID_ARGUMENT, "arrays exceeds the plan's max_arrays");
-    // Counting sort of array ids by exact length.
+    auto key_of = [by_bucket](int n) { return by_bucket ? ceil_log2(n) : n; };
+    // Counting sort of array ids by group key (empty arrays are skipped).
     int top = 0;
     for (int64_t a = 0; a < arrays; ++a) {
         const int n = h_offsets[a + 1] - h_offsets[a];
         if (n < 0) return set_error(B200S_ERR_INVALID_ARGUMENT, "offsets decrease");
-        top = std::max(top, n);
+        if (n > 0) top = std::max(top, key_of(n));
     }
     std::vector<int> start(size_t(top) + 2, 0);
-    for (int64_t a = 0; a < arrays; ++a) ++start[size_t(h_offsets[a + 1] - h_offsets[a]) + 1];
+    for (int64_t a = 0; a < arrays; ++a) {
+        const int n = h_offsets[a + 1] - h_offsets[a];
+        if (n > 0) ++start[size_t(key_of(n)) + 1];
+    }
     for (size_t i = 1; i < start.size(); ++i) start[i] += start[i - 1];
     std::vector<int> ids(size_t(std::max<int64_t>(arrays, 1)));
     std::vector<int> cursor(start.begin(), start.end() - 1);
-    for (int64_t a = 0; a < arrays; ++a) ids[size_t(cursor[size_t(h_offsets[a + 1] - h_offsets[a])]++)] = int(a);
+    for (int64_t a = 0; a < arrays; ++a) {
+        const int n = h_offsets[a + 1] - h_offsets[a];
+        if (n > 0) ids[size_t(cursor[size_t(key_of(n))]++)] = int(a);
+    }
     p->groups.clear();
-    for (int n = 1; n <= top; ++n) {
-        const int c = start[size_t(n) + 1] - start[size_t(n)];
+    for (int k = by_bucket ? 0 : 1; k <= top; ++k) {
+        const int c = start[size_t(k) + 1] - start[size_t(k)];
         if (!c) continue;
+        const long long len = by_bucket ? (1LL << k) : k;
         int persistent = 0;
-        const int entry = lookup_default_entry(p->dtype, p->stable, n, &persistent);
+        const int entry = lookup_default_entry(p->dtype, p->stable, len, &persistent);
         if (entry < 0) return set_error(B200S_ERR_UNSUPPORTED, "array longer than the largest tile");
-        p->groups.push_back({n, start[size_t(n)], c, entry, persistent});
+        p->groups.push_back({int(len), start[size_t(k)], c, entry, persistent});
     }
     cudaError_t e = cudaSetDevice(p->device);
-    if (e == cudaSuccess)
+    if (e == cudaSuccess && arrays > 0)
         e = cudaMemcpy(p->plain_ids, ids.data(), size_t(arrays) * sizeof(int), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_error(e, "upload plain ids");
     return B200S_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+b200s_status b200s_plan_prepare_plain(b200s_plan* p, const int32_t* h_offsets, int64_t arrays) {
+    return prepare_plain(p, h_offsets, arrays, false);
+}
+
+b200s_status b200s_plan_prepare_plain_buckets(b200s_plan* p, const int32_t* h_offsets, int64_t arrays) {
+    return prepare_plain(p, h_offsets, arrays, true);
 }
 
 b200s_status b200s_sort_ragged_plain(b200s_plan* p, const void* d_in, void* d_out, const int32_t* d_offsets,

@@ -33,6 +33,8 @@ constexpr int kRaggedLmin = 3;  // smallest bucket: W = 8
 struct RaggedCtl {
     int count[kMaxBuckets];    // arrays per bucket
     int cursor[kMaxBuckets];   // scatter cursors
+    int base[kMaxBuckets];     // first position of each bucket's ids in the id list
+    int dhead[kMaxBuckets];    // work queue heads of the dedicated bucket launches
     int head;                  // task queue head
     int too_long;              // arrays longer than every kernel (not sorted)
     int ocount[kMaxOverflow];  // arrays per cluster bucket
@@ -87,6 +89,7 @@ __global__ void k_bin_scatter(const int* __restrict__ off, int arrays, RaggedCtl
         int s = 0;
         for (int b = nb - 1; b >= 0; --b) {
             base[b] = s;
+            if (blockIdx.x == 0) ctl->base[b] = s;  // for the launches of dedicated buckets
             s += ctl->count[b];
         }
     }
@@ -178,27 +181,31 @@ __device__ __forceinline__ void ragged_task(const typename E::Mem* in, typename 
 }
 
 // NB buckets (W = 8 .. 8 << (NB-1)); bucket b uses family B (K = 2^LKB)
-// when bit b of family_mask is set, else family A (K = 2^LKA).  SB: one
-// shared-memory buffer per team (two barriers per shared-memory layer, half
-// the shared memory); MINB: CTAs per SM the register budget is sized for.
+// when bit b of family_mask is set, else family A (K = 2^LKA); buckets whose
+// bit is set in dedicated_mask are left to their own launches (their ids stay
+// in the list at ctl->base[b]).  SB: one shared-memory buffer per team (two
+// barriers per shared-memory layer, half the shared memory); MINB: CTAs per
+// SM the register budget is sized for.
 template <class E, int CTA, int NB, int LKA, int LKB, bool SB, int MINB>
 __global__ void __launch_bounds__(CTA, MINB) k_sort_ragged(const typename E::Mem* in, typename E::Mem* out,
                                                         const int* __restrict__ off,
                                                         const int* __restrict__ ids, RaggedCtl* ctl,
-                                                        unsigned family_mask) {
+                                                        unsigned family_mask, unsigned dedicated_mask) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_first[NB], s_tasks[NB], s_base[NB], s_count[NB];
     __shared__ int s_total, s_task;
     if (threadIdx.x == 0) {
         int task = 0, base = 0;
         for (int b = NB - 1; b >= 0; --b) {
+            // dedicated buckets get no tasks here, but their ids still occupy
+            // the list, so the bases count them
             const int c = ctl->count[b];
             const int L = b + kRaggedLmin;
             const int lk = family_lk(L, ((family_mask >> b) & 1u) ? LKB : LKA, log2_const(CTA));
             const int tpa = 1 << (L - lk);
             const int apt = CTA / tpa;
             s_first[b] = task;
-            s_tasks[b] = (c + apt - 1) / apt;
+            s_tasks[b] = ((dedicated_mask >> b) & 1u) ? 0 : (c + apt - 1) / apt;
             s_base[b] = base;
             s_count[b] = c;
             task += s_tasks[b];
@@ -253,20 +260,39 @@ constexpr size_t ragged_smem() {
     return best;
 }
 
-// Plain per-length launches: every array of the id list has the same length
-// class; one group per array, grid covers the list.
+// Launches over an id list: every array of the list fits the tile; one group
+// per array.  With d_count null the grid strides over `count` arrays.
+// Otherwise (a dedicated bucket of a ragged plan) the count and the list's
+// first position are read on the device, so that a captured launch sorts
+// whatever the binning put into its bucket, and the resident CTAs pull groups
+// of arrays from the queue at d_head (one atomicAdd per group), which keeps
+// them busy when the arrays' lengths, and so their costs, differ.
 template <class E, class S, int CTA, bool SB = false>
 __global__ void __launch_bounds__(CTA) k_sort_idlist(const typename E::Mem* in, typename E::Mem* out,
                                                      const int* __restrict__ off, const int* __restrict__ ids,
-                                                     int count) {
+                                                     int count, const int* d_count, const int* d_base,
+                                                     int* d_head) {
     using R = typename E::Reg;
+    __shared__ int s_next;
+    if (d_count) {
+        count = *d_count;
+        ids += *d_base;
+    }
     constexpr int APC = CTA / S::TPA;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* cur = reinterpret_cast<R*>(smem_raw);
     R* nxt = SB ? cur : cur + S::W;  // the launch passes 1 or 2 buffers of W elements
     const int slot = int(threadIdx.x) / S::TPA;
     const int t = int(threadIdx.x) % S::TPA;
-    for (long long first = (long long)blockIdx.x * APC; first < count; first += (long long)gridDim.x * APC) {
+    long long first = (long long)blockIdx.x * APC;
+    for (;;) {
+        if (d_head) {
+            if (threadIdx.x == 0) s_next = atomicAdd(d_head, APC);
+            __syncthreads();
+            first = s_next;
+            __syncthreads();
+        }
+        if (first >= count) break;  // uniform across the CTA
         const long long g = first + slot;
         int na = 0;
         long long start = 0;
@@ -280,6 +306,7 @@ __global__ void __launch_bounds__(CTA) k_sort_idlist(const typename E::Mem* in, 
         if constexpr (SB) network<E, S>(v, t, cur, nxt, CtaBarrierSingle{}, na);
         else network<E, S>(v, t, cur, nxt, CtaBarrier{}, na);
         store_tile<E, S::K>(v, out + start, t * S::K, na);
+        if (!d_head) first += (long long)gridDim.x * APC;
     }
 }
 

@@ -19,6 +19,11 @@ using AttrQuery = cudaError_t (*)(cudaFuncAttributes* attr);
 // Launch over a list of array ids of a CSR batch (plain per-length launches).
 using ListLaunch = cudaError_t (*)(const void* in, void* out, const int* d_off, const int* d_ids,
                                    int count, cudaStream_t stream);
+// The same with the count and the list's first position read on the device
+// (a dedicated bucket of a ragged plan): at most max_count arrays.
+using ListLaunchDev = cudaError_t (*)(const void* in, void* out, const int* d_off, const int* d_ids,
+                                      const int* d_count, const int* d_base, int* d_head, int max_count,
+                                      cudaStream_t stream);
 
 struct KernelEntry {
     int dtype;        // b200s_dtype
@@ -37,6 +42,7 @@ struct KernelEntry {
     // with the count read on the device (at most max_count).
     cudaError_t (*launch_cluster_list)(const void* in, void* out, const int* d_off, const int* d_ids,
                                        const int* d_count, int max_count, cudaStream_t stream);
+    ListLaunchDev launch_list_dev;  // single-CTA tiles only (null for cluster kernels)
 };
 
 void register_i32(std::vector<KernelEntry>& out);
@@ -52,7 +58,8 @@ struct RaggedCtl;
 
 // The persistent ragged kernel of one element type.
 using RaggedLaunch = cudaError_t (*)(const void* in, void* out, const int* d_off, const int* d_ids,
-                                     RaggedCtl* ctl, unsigned family_mask, int grid, cudaStream_t stream);
+                                     RaggedCtl* ctl, unsigned family_mask, unsigned dedicated_mask, int grid,
+                                     cudaStream_t stream);
 struct RaggedEntry {
     int dtype;
     int stable;
@@ -60,7 +67,7 @@ struct RaggedEntry {
     int nb;           // buckets: W = 8 .. 8 << (nb - 1)
     int lka, lkb;     // log2 elements per thread of shape families A and B
     size_t smem;      // dynamic shared memory bytes
-    RaggedLaunch launch;
+    RaggedLaunch launch;  // family_mask, dedicated_mask: see k_sort_ragged
     int (*resident_per_sm)();  // CTAs per SM (occupancy), 0 on error
 };
 

@@ -8,9 +8,10 @@ compiled single-CTA tile of that W in each launch form it has (0 one slot per
 array, 1 persistent with register prefetch, 2 persistent TMA pipeline, 3
 transposed network) on a full-length batch of about 4 M elements, checks the
 output, and keeps the fastest as the packed row.  For the ragged kernel it
-times, per bucket L, a batch whose lengths all fall in that bucket with the
-bucket's shape family A and with family B, and keeps the faster as the
-ragged row.
+times, per bucket L, a batch whose lengths all fall in that bucket in the
+persistent kernel with the bucket's shape family A, with family B, and as a
+launch of its own (the tabled tile of its working length, beside the
+persistent kernel), and keeps the fastest as the ragged row.
 
 Timing (devtime.batched_us): each pass evicts L2, then runs one launch on
 each of several buffer sets (at least twice the L2 in total) back to back
@@ -36,6 +37,9 @@ import workloads  # noqa: E402
 
 TARGET_ELEMS = 1 << 22
 FORM_NAMES = {0: "one-shot", 1: "prefetch", 2: "TMA", 3: "transposed"}
+# ragged rows: 0 / 1 run the bucket in the persistent kernel with shape family
+# A / B; 2 gives the bucket its own launch of the tabled tile of its length
+FAMILY_NAMES = {0: "persistent A", 1: "persistent B", 2: "own launch"}
 
 
 def _keys(dtype, arr):
@@ -110,7 +114,7 @@ def tune_ragged(dtype, flags, flush, passes, log, summary):
         outs = [torch.empty_like(src) for _ in range(sets)]
         d_off = torch.from_numpy(off.astype(np.int32)).cuda()
         res = {}
-        for fam in (0, 1):
+        for fam in (0, 1, 2):
             with tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False) as f:
                 f.write("r,%d,%d,%d,%d\n" % (dtype, flags, L, fam))
             bs.load_tile_table(f.name)
@@ -125,11 +129,12 @@ def tune_ragged(dtype, flags, flush, passes, log, summary):
                 p.close()
             log("ragged dtype=%d flags=%d W=%d family=%d: %.2f us (spread %.1f %%)"
                 % (dtype, flags, 1 << L, fam, res[fam][0], 100 * res[fam][1]))
-        fam = min(res, key=lambda k: res[k][0])
-        rows.append("r,%d,%d,%d,%d  # %.2f us (spread %.1f %%) vs %.2f us"
-                    % (dtype, flags, L, fam, res[fam][0], 100 * res[fam][1], res[1 - fam][0]))
-        summary.append(("ragged", dtype, flags, 1 << L, arrays, "family %s" % "AB"[fam], res[fam][0], res[fam][1],
-                        "family %s" % "AB"[1 - fam], res[1 - fam][0]))
+        order = sorted(res, key=lambda k: res[k][0])
+        fam, second = order[0], order[1]
+        rows.append("r,%d,%d,%d,%d  # %.2f us (spread %.1f %%) vs %.2f us (%s)"
+                    % (dtype, flags, L, fam, res[fam][0], 100 * res[fam][1], res[second][0], FAMILY_NAMES[second]))
+        summary.append(("ragged", dtype, flags, 1 << L, arrays, FAMILY_NAMES[fam], res[fam][0], res[fam][1],
+                        FAMILY_NAMES[second], res[second][0]))
         del ins, outs, src
         torch.cuda.empty_cache()
         L += 1
@@ -181,7 +186,8 @@ def main():
                                                          "%Y-%m-%d %H:%M UTC"), bs.version()))
         f.write("# packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps,form (0 one-shot, 1 prefetch, 2 TMA, "
                 "3 transposed)\n")
-        f.write("# ragged rows: r,dtype,flags,log2_w,family (0: larger per-thread tile, 1: smaller)\n")
+        f.write("# ragged rows: r,dtype,flags,log2_w,family (0: persistent, larger per-thread tile; 1: persistent, "
+                "smaller; 2: own launch of the tabled tile)\n")
         for ln in lines:
             f.write(ln + "\n")
     if args.summary:

@@ -94,8 +94,10 @@ typedef struct b200s_tile {
                             array is whole 128-byte rows, at most 256, and the buffers are
                             16-byte aligned; form 0 otherwise); 3: transposed network, every
                             comparator layer in registers with the tile re-laid out through
-                            shared memory between register windows (single-warp int32-key
-                            tiles of 32 keys per lane; form 0 for other tiles) */
+                            shared memory between register windows (single-warp tiles of
+                            int32 and uint64 keys, IntAndData records and stable records up
+                            to W = 1024, with element-aligned buffers; b200s_tile_info's
+                            xpose_form tells which; form 0 otherwise) */
     int32_t log2_ctas;   /* CTAs per array: 0 for single-CTA tiles (cluster tiles of one
                             CTA exist only where no single-CTA tile of that shape does) */
 } b200s_tile;
@@ -178,6 +180,11 @@ b200s_status b200s_plan_too_long(b200s_plan* plan, void* stream, int64_t* count)
  * length on the host (from host offsets) and uploads the id lists; each sort
  * then issues one launch per distinct length. */
 b200s_status b200s_plan_prepare_plain(b200s_plan* plan, const int32_t* h_offsets, int64_t arrays);
+/* The same grouped by power-of-two working length instead of exact length:
+ * one launch per length class (W/2, W] with the tile of W, about log2 of the
+ * longest array launches; a plain comparator without the launch count of the
+ * per-length form.  b200s_sort_ragged_plain then runs these groups. */
+b200s_status b200s_plan_prepare_plain_buckets(b200s_plan* plan, const int32_t* h_offsets, int64_t arrays);
 b200s_status b200s_sort_ragged_plain(b200s_plan* plan, const void* d_in, void* d_out,
                                      const int32_t* d_offsets, void* stream);
 int32_t b200s_plan_plain_launches(const b200s_plan* plan);

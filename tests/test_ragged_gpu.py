@@ -124,3 +124,55 @@ def test_full_ragged_batch_200000_arrays():
     got, too_long = run(dtype, 0, data, off, "graph", reps=2)
     assert too_long == 0
     check(dtype, 0, data, off, got)
+
+
+def _route(dtype, flags, rows):
+    """Load ragged table rows (log2 W, family) for dtype/flags; family 2 gives
+    the bucket its own launch of the tabled tile."""
+    import tempfile
+    with tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False) as f:
+        for L, fam in rows:
+            f.write("r,%d,%d,%d,%d\n" % (dtype, flags, L, fam))
+    try:
+        bs.load_tile_table(f.name)
+    finally:
+        import os
+        os.unlink(f.name)
+
+
+@pytest.mark.parametrize("dtype,flags", [(bs.I32, 0), (bs.I32_I32, 0), (bs.I32_I32, bs.STABLE), (bs.U64, 0),
+                                         (bs.U64_I32, 0)])
+def test_buckets_with_their_own_launch_match_the_oracle(dtype, flags):
+    # every persistent-range bucket dedicated, then every other one, then none:
+    # the same output, record for record, in the graph and the direct form
+    top = bs.ragged_max_length(dtype, flags)
+    lengths = workloads.ragged_lengths(4000, max_len=min(top, 12000), seed=31)
+    lengths[::29] = 0
+    data, off = workloads.make_ragged(dtype, lengths, "distinct16", seed=31, extremes=True)
+    exp = expected(dtype, flags, data, off)
+    Ls = list(range(3, 15))
+    try:
+        for routing in ([(L, 2) for L in Ls], [(L, 2 if L % 2 else 0) for L in Ls]):
+            _route(dtype, flags, routing)
+            for form in ("graph", "direct"):
+                got, too_long = run(dtype, flags, data, off, form, reps=2)
+                assert too_long == 0
+                assert np.array_equal(got, exp), (routing[:2], form)
+            # the allocation-free path follows the same routing
+            import ctypes
+            import torch
+            fn = bs.declare("b200s_sort_ragged_noalloc", ctypes.c_int,
+                            [ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                             ctypes.c_int64, ctypes.c_void_p])
+            d_in = to_device(data)
+            d_out = empty_device(d_in.numel())
+            d_off = torch.from_numpy(off.astype(np.int32)).cuda()
+            assert fn(dtype, flags, d_in.data_ptr(), d_out.data_ptr(), d_off.data_ptr(), len(off) - 1,
+                      stream_handle()) == 0
+            torch.cuda.synchronize()
+            assert np.array_equal(from_device(d_out[:data.nbytes], bs.NP_DTYPES[dtype]), exp)
+    finally:
+        _route(dtype, flags, [(L, 0) for L in Ls])
+        import os
+        table = os.path.join(os.path.dirname(bs.LIB_PATH), "tune", "b200_table.csv")
+        bs.load_tile_table(table)   # back to the shipped table
