@@ -13,11 +13,15 @@ evicted from the 126 MB L2 (batches larger than L2 use one set).  Rank 0
 prints one JSON line.
 
 Workloads: int32_4096x1024 (default), records_n{32,129,256,1000,2048,4096}
-(IntAndData records, 4194304 per batch), ragged_200000 (200000 CSR arrays,
-lengths log-uniform in [1, 8192], records; the persistent bucketed launch
-replayed from its CUDA graph, with the plain per-length launches timed
-beside it), cluster_256x65536 / cluster_u64_256x65536 (256 arrays of 65536
-records with int32 / uint64 keys, one 8-CTA thread-block cluster per array),
+(IntAndData records, 4194304 per batch; --distribution picks one of the
+nine seeded distributions, --sorted-check sets B200S_SORTED_CHECK),
+ragged_200000 (200000 CSR arrays,
+lengths log-uniform in [1, 8192], records; the plan's launch sequence
+replayed from its CUDA graph, with one launch per length class and the
+plain per-length launches timed beside it), cluster_256x65536 /
+cluster_u64_256x65536 (256 arrays of 65536 records with int32 / uint64
+keys, one thread-block cluster per array: 4 CTAs of 1024 threads / 8 CTAs
+of 512),
 serving (a stream of sort requests of 16 .. 65536 records into the
 continuous-batching server under a 16 GB device budget: peak sustained keys/s
 in closed loop, then Poisson arrival rates with p50/p99/p99.9 latency, each
