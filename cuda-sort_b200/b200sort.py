@@ -115,6 +115,8 @@ _SIGNATURES = {
     "b200s_ragged_max_length": (ctypes.c_int32, [ctypes.c_int, ctypes.c_uint32]),
     "b200s_sort_ragged": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_int64, ctypes.c_void_p]),
+    "b200s_sort_ragged_hinted": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     "b200s_plan_too_long": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
     "b200s_plan_prepare_plain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]),
     "b200s_sort_ragged_plain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -277,6 +279,14 @@ class Plan:
     def sort(self, d_in, d_out, d_offsets, arrays, stream=0):
         return check(lib().b200s_sort_ragged(self._h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out),
                                              ctypes.c_void_p(d_offsets), arrays, ctypes.c_void_p(stream)))
+
+    def sort_hinted(self, d_in, d_out, d_offsets, h_offsets_int32, stream=0):
+        """sort() with the host copy of the offsets: a plan made with
+        PLAN_NO_GRAPH launches only the length classes the batch holds."""
+        off = np.ascontiguousarray(h_offsets_int32, dtype=np.int32)
+        return check(lib().b200s_sort_ragged_hinted(self._h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out),
+                                                    ctypes.c_void_p(d_offsets), ctypes.c_void_p(off.ctypes.data),
+                                                    len(off) - 1, ctypes.c_void_p(stream)))
 
     def too_long(self, stream=0):
         c = ctypes.c_int64(0)

@@ -130,8 +130,11 @@ struct b200s_plan {
 
 namespace {
 
+// present / over_present: bit b set when bucket b (cluster class i) may hold
+// an array; classes with a launch of their own are skipped when their bit is
+// clear (all ones: launch everything, as a graph must).
 b200s_status record_sequence(b200s_plan* p, const void* in, void* out, const int* off, int arrays,
-                             cudaStream_t st) {
+                             cudaStream_t st, uint32_t present = ~0u, uint32_t over_present = ~0u) {
     cudaError_t e = cudaMemsetAsync(p->ctl, 0, sizeof(RaggedCtl), st);
     if (e != cudaSuccess) return cuda_error(e, "ragged control reset");
     const int bin_threads = 256;
@@ -155,16 +158,17 @@ b200s_status record_sequence(b200s_plan* p, const void* in, void* out, const int
         return p->side[s];
     };
     int k = 0;
-    for (int i = p->spec.n_over - 1; i >= 0; --i, ++k) {
+    for (int i = p->spec.n_over - 1; i >= 0; --i) {
+        if (!((over_present >> i) & 1u)) continue;
         const KernelEntry& ke = registry()[size_t(p->over_entry[i])];
-        cudaStream_t ss = side_stream(k);
+        cudaStream_t ss = side_stream(k++);
         if (!ss) return cuda_error(e, "fork");
         e = ke.launch_cluster_list(in, out, off, p->oids + size_t(i) * p->spec.stride, &p->ctl->ocount[i],
                                    max_count, ss);
         if (e != cudaSuccess) return cuda_error(e, "cluster bucket launch");
     }
     for (int b = p->spec.nb - 1; b >= 0; --b) {
-        if (!((p->dedicated_mask >> b) & 1u)) continue;
+        if (!((p->dedicated_mask >> b) & (present >> b) & 1u)) continue;
         const KernelEntry& ke = registry()[size_t(p->dedicated_entry[b])];
         cudaStream_t ss = side_stream(k++);
         if (!ss) return cuda_error(e, "fork");
@@ -172,7 +176,8 @@ b200s_status record_sequence(b200s_plan* p, const void* in, void* out, const int
                                max_count, ss);
         if (e != cudaSuccess) return cuda_error(e, "dedicated bucket launch");
     }
-    if (p->dedicated_mask != (1u << p->spec.nb) - 1u) {
+    const uint32_t all = (1u << p->spec.nb) - 1u;
+    if (present & all & ~p->dedicated_mask) {
         e = p->rk->launch(in, out, off, p->ids, p->ctl, p->family_mask, p->dedicated_mask, p->grid, st);
         if (e != cudaSuccess) return cuda_error(e, "ragged sort launch");
     }
@@ -344,6 +349,31 @@ b200s_status b200s_sort_ragged(b200s_plan* p, const void* d_in, void* d_out, con
     e = cudaGraphLaunch(p->exec, st);
     if (e != cudaSuccess) return cuda_error(e, "graph launch");
     return B200S_OK;
+}
+
+b200s_status b200s_sort_ragged_hinted(b200s_plan* p, const void* d_in, void* d_out, const int32_t* d_offsets,
+                                      const int32_t* h_offsets, int64_t arrays, void* stream) {
+    if (!p) return set_error(B200S_ERR_INVALID_ARGUMENT, "null plan");
+    if (!h_offsets || !(p->flags & B200S_PLAN_NO_GRAPH))
+        return b200s_sort_ragged(p, d_in, d_out, d_offsets, arrays, stream);
+    if (arrays < 0 || arrays > p->max_arrays)
+        return set_error(B200S_ERR_INVALID_ARGUMENT, "arrays exceeds the plan's max_arrays");
+    if (arrays == 0) return B200S_OK;
+    if (!d_in || !d_out || !d_offsets) return set_error(B200S_ERR_INVALID_ARGUMENT, "null buffer");
+    // the classes the batch holds, by the binning kernel's rule
+    uint32_t present = 0, over_present = 0;
+    for (int64_t a = 0; a < arrays; ++a) {
+        const int n = h_offsets[a + 1] - h_offsets[a];
+        if (n <= 0) continue;
+        const int l = n <= 1 ? 0 : 32 - __builtin_clz(unsigned(n - 1));
+        const int b = (l > kRaggedLmin ? l : kRaggedLmin) - kRaggedLmin;
+        if (b < p->spec.nb) present |= 1u << b;
+        else if (l - p->spec.over_lo < p->spec.n_over) over_present |= 1u << (l - p->spec.over_lo);
+    }
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    return record_sequence(p, d_in, d_out, d_offsets, int(arrays), static_cast<cudaStream_t>(stream), present,
+                           over_present);
 }
 
 b200s_status b200s_plan_too_long(b200s_plan* p, void* stream, int64_t* count) {

@@ -200,8 +200,10 @@ public:
         k_stage<<<chunks, kStageThreads, 0, s.stream>>>(d_desc, count, arena, eb_, pad0_, pad1_, 0);
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "stage-in launch", err);
         void* region = arena + region_elem * eb_;
-        const b200s_status st = b200s_sort_ragged(s.plan, region, region, reinterpret_cast<const int32_t*>(s.d_meta),
-                                                  count, s.stream);
+        // the host copy of the offsets lets the plan skip the classes this batch has no array in
+        const b200s_status st = b200s_sort_ragged_hinted(s.plan, region, region,
+                                                         reinterpret_cast<const int32_t*>(s.d_meta), off, count,
+                                                         s.stream);
         if (st != B200S_OK) {
             *err = std::string("server batch sort: ") + b200s_last_error();
             return st;

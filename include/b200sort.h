@@ -171,9 +171,22 @@ b200s_status b200s_plan_create(b200s_plan** out, b200s_dtype dtype, uint32_t fla
 b200s_status b200s_plan_destroy(b200s_plan* plan);
 /* Longest array the ragged path sorts; longer arrays are counted, not sorted. */
 int32_t b200s_ragged_max_length(b200s_dtype dtype, uint32_t flags);
-/* One persistent, length-bucketed launch (graph-replayed). */
+/* The plan's launch sequence: binning, then the persistent length-bucketed
+ * kernel on `stream`, with the length classes that the tile table gives a
+ * launch of their own and the cluster classes above the persistent kernel's
+ * range on side streams, joined before return (graph-replayed unless
+ * B200S_PLAN_NO_GRAPH). */
 b200s_status b200s_sort_ragged(b200s_plan* plan, const void* d_in, void* d_out, const int32_t* d_offsets,
                                int64_t arrays, void* stream);
+/* b200s_sort_ragged for a caller that also holds the offsets on the host
+ * (h_offsets: the same arrays + 1 values as d_offsets, read during the call).
+ * A B200S_PLAN_NO_GRAPH plan then issues only the launches of the length
+ * classes the batch holds: a launch of its own or a cluster class that no
+ * array falls in is skipped, and so is the persistent kernel when every
+ * array is in such a class.  Results equal b200s_sort_ragged's.  A graph plan
+ * (or h_offsets == NULL) runs b200s_sort_ragged. */
+b200s_status b200s_sort_ragged_hinted(b200s_plan* plan, const void* d_in, void* d_out, const int32_t* d_offsets,
+                                      const int32_t* h_offsets, int64_t arrays, void* stream);
 /* Arrays of the last b200s_sort_ragged that exceeded b200s_ragged_max_length
  * (synchronises `stream`). */
 b200s_status b200s_plan_too_long(b200s_plan* plan, void* stream, int64_t* count);

@@ -176,3 +176,43 @@ def test_buckets_with_their_own_launch_match_the_oracle(dtype, flags):
         import os
         table = os.path.join(os.path.dirname(bs.LIB_PATH), "tune", "b200_table.csv")
         bs.load_tile_table(table)   # back to the shipped table
+
+
+@pytest.mark.parametrize("dtype,flags", [(bs.I32, 0), (bs.I32_I32, 0), (bs.U64_I32, bs.STABLE)])
+def test_hinted_sort_launches_only_the_classes_present(dtype, flags):
+    # a direct plan told the host offsets skips the empty classes: batches with
+    # only short arrays, only long ones, only cluster-range ones, a mix, and
+    # only empty arrays, under the shipped routing and with every other
+    # persistent-range class on a launch of its own
+    import os
+    import torch
+    top = bs.ragged_max_length(dtype, flags)
+    rng = np.random.default_rng(77)
+    cases = [rng.integers(1, 33, 300), rng.integers(2049, 8193, 40), rng.integers(16385, top + 1, 6),
+             np.concatenate([rng.integers(1, 17, 50), rng.integers(4097, 8193, 8), rng.integers(16385, top + 1, 3)]),
+             np.array([0] * 19 + [5]), np.array([1000])]
+    Ls = list(range(3, 15))
+    plan = bs.Plan(dtype, 400, flags | bs.PLAN_NO_GRAPH)
+    st = stream_handle()
+    try:
+        for routing in (None, [(L, 2 if L % 2 else 0) for L in Ls]):
+            if routing:
+                plan.close()
+                _route(dtype, flags, routing)
+                plan = bs.Plan(dtype, 400, flags | bs.PLAN_NO_GRAPH)
+            for i, lengths in enumerate(cases):
+                lengths = rng.permutation(lengths.astype(np.int64))
+                data, off = workloads.make_ragged(dtype, lengths, "uniform", seed=i, extremes=True)
+                exp = expected(dtype, flags, data, off)
+                d_in = to_device(data)
+                d_out = to_device(np.zeros_like(data))
+                d_off = torch.from_numpy(off.astype(np.int32)).cuda()
+                plan.sort_hinted(d_in.data_ptr(), d_out.data_ptr(), d_off.data_ptr(), off.astype(np.int32), st)
+                torch.cuda.synchronize()
+                assert plan.too_long(st) == 0
+                got = from_device(d_out[:data.nbytes], bs.NP_DTYPES[dtype])
+                assert np.array_equal(got, exp), (routing is not None, i)
+    finally:
+        plan.close()
+        _route(dtype, flags, [(L, 0) for L in Ls])
+        bs.load_tile_table(os.path.join(os.path.dirname(bs.LIB_PATH), "tune", "b200_table.csv"))
