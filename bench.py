@@ -656,9 +656,15 @@ def run_gpu(args, wl):
         keys_in = data if dtype in (bs.I32, bs.U64) else data["key"]
         keys_out = got if dtype in (bs.I32, bs.U64) else got["key"]
         verified = bool(np.array_equal(keys_out.reshape(arrays, n), np.sort(keys_in.reshape(arrays, n), axis=1)))
-        if form == 3 and not bs.tile_info(dtype, n, flags, eff).xpose_form:
+        info = bs.tile_info(dtype, n, flags, eff)
+        cluster = info.arrays_per_cta == 0
+        if form == 3 and not info.xpose_form:
             form = 0
-        kernel = {0: "k_sort_packed", 1: "k_sort_packed_pf", 2: "k_sort_packed_tma", 3: "k_sort_xpose"}[form]
+        if form == 3:
+            kernel = "k_sort_cluster_xc" if cluster else "k_sort_packed_xc" if eff.log2_warps > 0 else "k_sort_xpose"
+        else:
+            kernel = "k_sort_cluster" if cluster else {0: "k_sort_packed", 1: "k_sort_packed_pf",
+                                                       2: "k_sort_packed_tma"}[form]
         launches = args.steps
         if ctx.world == 1 and not args.no_baselines:
             extra["baselines"] = gpu_baselines(ctx, wl, data, host, eff)

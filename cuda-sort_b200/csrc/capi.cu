@@ -67,6 +67,10 @@ const std::vector<KernelEntry>& registry() {
         register_cluster_keys(v);
         register_cluster_rec(v);
         register_cluster_u64rec(v);
+        register_xc_keys(v);
+        register_xc_rec(v);
+        register_xc_cluster_rec(v);
+        register_xc_u64rec(v);
         return v;
     }();
     return all;
@@ -181,7 +185,8 @@ bool valid_dtype(int d) { return d >= 0 && d <= 3; }
 namespace {
 
 // Tile table CSV: '#' comments; packed rows dtype,flags,log2_w,log2_items,
-// log2_lanes,log2_warps[,persistent]; ragged rows r,dtype,flags,log2_w,family.
+// log2_lanes,log2_warps[,persistent[,log2_ctas]]; ragged rows
+// r,dtype,flags,log2_w,family.
 b200s_status parse_table_file(const char* path, TableRows* out) {
     std::ifstream f(path);
     if (!f) return set_error(B200S_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path);
@@ -204,16 +209,17 @@ b200s_status parse_table_file(const char* path, TableRows* out) {
             out->ragged.push_back({d, effective_stable(d, uint32_t(fl)), w, fam});
             continue;
         }
-        int d, fl, w, lk, lg, lw, pers = 0;
+        int d, fl, w, lk, lg, lw, pers = 0, lc = 0;
         if (!(ss >> d >> fl >> w >> lk >> lg >> lw))
             return set_error(B200S_ERR_INVALID_ARGUMENT,
-                             "tile table line " + std::to_string(lineno) + ": expected 6 or 7 integers");
+                             "tile table line " + std::to_string(lineno) + ": expected 6 to 8 integers");
         if (!(ss >> pers)) pers = 0;
+        else if (!(ss >> lc)) lc = 0;
         if (!valid_dtype(d) || w < 0 || w > kMaxLog2W)
             return set_error(B200S_ERR_INVALID_ARGUMENT,
                              "tile table line " + std::to_string(lineno) + ": bad dtype or log2_w");
         const int stable = effective_stable(d, uint32_t(fl));
-        const b200s_tile tile{lk, lg, lw, 0, 0, 0};
+        const b200s_tile tile{lk, lg, lw, 0, 0, lc};
         const int idx = lookup_tile(d, stable, tile);
         if (idx < 0 || registry()[size_t(idx)].log2w < w)
             return set_error(B200S_ERR_UNSUPPORTED,
@@ -292,6 +298,11 @@ b200s_status launch_packed(int idx, int persistent, const void* in, void* out, i
             x = nullptr;  // element-wide accesses need element-aligned buffers: form 0 instead
         if (x) {
             const cudaError_t err = x->launch(in, out, n, arrays, st, opts);
+            if (err != cudaSuccess) return cuda_error(err, "transposed-network sort kernel launch");
+            return B200S_OK;
+        }
+        if (!xpose_for(e) && e.launch_xc) {  // multi-warp and cluster tiles
+            const cudaError_t err = e.launch_xc(in, out, n, arrays, 0, st, opts);
             if (err != cudaSuccess) return cuda_error(err, "transposed-network sort kernel launch");
             return B200S_OK;
         }
@@ -482,7 +493,7 @@ b200s_status b200s_tile_info_get(b200s_dtype dtype, uint32_t flags, const b200s_
     out->arrays_per_cta = e.lc >= 0 ? 0 : e.apc;
     static const char aligned[16] = {};  // any 16-byte aligned address stands for the buffers
     out->tma_form = tma_for(e, aligned, aligned, std::max(1, n), 1) ? 1 : 0;
-    out->xpose_form = xpose_for(e) ? 1 : 0;
+    out->xpose_form = (xpose_for(e) || e.launch_xc) ? 1 : 0;
     return B200S_OK;
 }
 

@@ -67,7 +67,7 @@ __device__ __forceinline__ void xc_put(const typename E::Reg (&v)[1 << LK], cons
     const int bm = MIR ? xc_base<LK, A, true>(t) : bp;
     sfor<0, (1 << LK)>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
-        sm[((MIR && (q & H)) ? bm : bp) + xc_off<LK, A, MIR>(q)] = v[q];
+        sh_st(&sm[((MIR && (q & H)) ? bm : bp) + xc_off<LK, A, MIR>(q)], v[q]);
     });
 }
 template <class E, int LK, int A, bool MIR>
@@ -77,7 +77,7 @@ __device__ __forceinline__ void xc_get(typename E::Reg (&v)[1 << LK], const int 
     const int bm = MIR ? xc_base<LK, A, true>(t) : bp;
     sfor<0, (1 << LK)>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
-        v[q] = sm[((MIR && (q & H)) ? bm : bp) + xc_off<LK, A, MIR>(q)];
+        v[q] = sh_ld(&sm[((MIR && (q & H)) ? bm : bp) + xc_off<LK, A, MIR>(q)]);
     });
 }
 
@@ -169,46 +169,110 @@ constexpr int xc_smem_elems() {
     return xp_addr<LK>((1 << LOGW) - 1) + 1;
 }
 
-// Cross-CTA layer of a cluster stage: partner of (rank, local index i) is
-// (rank ^ cm, reflect ? i ^ (W - 1) : i); natural layout; the slice is
-// published at its logical addresses.
+// Cross-CTA layer of a cluster stage, in window layout LT (register q of
+// thread t holds local index (q << LT) | t, so the lanes of a warp read 32
+// consecutive elements of the partner's slice): the partner of (rank, local
+// index i) is (rank ^ cm, reflect ? i ^ (W - 1) : i).  The slice is
+// published at its logical addresses, then read back from the partner CTA.
 template <class E, int LK, int LT, bool REFLECT>
 __device__ __forceinline__ void xc_cluster_layer(typename E::Reg (&v)[1 << LK], const int t, const int rank,
                                                  const int cm, const bool upper, typename E::Reg* sm) {
     using R = typename E::Reg;
-    constexpr int K = 1 << LK;
+    constexpr int K = 1 << LK, T = 1 << LT;
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
-    xc_put<E, LK, 0, false>(v, t, sm);
+    xc_put<E, LK, LT, false>(v, t, sm);
     cluster.sync();
     const R* remote = cluster.map_shared_rank(sm, rank ^ cm);
-    const int pb = xp_addr<LK>((REFLECT ? ((1 << LT) - 1 - t) : t) << LK);
+    const int pb = xp_addr<LK>(REFLECT ? T - 1 - t : t);
     sfor<0, K>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
-        const R b = remote[pb + xp_addr<LK>(REFLECT ? K - 1 - q : q)];
+        const R b = sh_ld(&remote[pb + xp_addr<LK>((REFLECT ? K - 1 - q : q) << LT)]);
         v[q] = E::pick(v[q], b, upper);
     });
     cluster.sync();
 }
 
 // The network of an array held by a cluster of 2^LC CTAs of 2^LT threads
-// (slice of 2^(LK+LT) elements per CTA): local stages, then per cluster
-// stage its cross-CTA layers and the local merges as a window chain.
+// (slice of 2^(LK+LT) elements per CTA): the local stages, then per cluster
+// stage its cross-CTA layers in window layout LT, the merges on the slice's
+// top LK bits in the same registers, and the rest as a window chain.
 template <class E, int LK, int LT, int LC>
 __device__ __forceinline__ void xc_cluster_network(typename E::Reg (&v)[1 << LK], const int t, const int rank,
                                                    typename E::Reg* sm) {
     constexpr int LOCAL = LK + LT;
     const CtaBarrier bar{};
     xc_network<E, LK, LOCAL>(v, t, sm, bar);
-    __syncthreads();  // every thread's last read of the region is done before it is published
 #pragma unroll 1
     for (int st = LOCAL; st < LOCAL + LC; ++st) {
+        xc_move<E, LK, 0, false, LT, false>(v, t, sm, bar);
+        __syncthreads();  // every thread has read the region before it is published again
         xc_cluster_layer<E, LK, LT, true>(v, t, rank, (2 << (st - LOCAL)) - 1, (rank >> (st - LOCAL)) & 1, sm);
 #pragma unroll 1
         for (int j = st - 1; j >= LOCAL; --j)
             xc_cluster_layer<E, LK, LT, false>(v, t, rank, 1 << (j - LOCAL), (rank >> (j - LOCAL)) & 1, sm);
-        xc_chain<E, LK, 0, false, LOCAL - 1>(v, t, sm, bar);
+        // merges on local bits LOCAL-1 .. LT: the registers of window LT
+        xc_reg_merges<E, LK, LK - 1>(v);
+        xc_chain<E, LK, LT, false, LT - 1>(v, t, sm, bar);
+    }
+}
+
+// One array per CTA of S::TPA threads (S::LW > 0), the grid striding over the
+// batch; arguments and the sorted check as k_sort_packed's.
+template <class E, class S, int MINB = 1>
+__global__ void __launch_bounds__(S::TPA, MINB) k_sort_packed_xc(const typename E::Mem* in, typename E::Mem* out,
+                                                                int n, long long arrays, unsigned opts) {
+    using R = typename E::Reg;
+    static_assert(S::LW > 0, "the transposed network of one warp is xpose.cuh's");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* sm = reinterpret_cast<R*>(smem_raw);
+    const int t = int(threadIdx.x);
+    for (long long a = blockIdx.x; a < arrays; a += gridDim.x) {
+        const long long off = a * (long long)n;
+        R v[S::K];
+        load_tile<E, S::K>(v, in + off, t * S::K, n);
+        const bool skip = (opts & kOptSortedCheck) && team_in_order<E, S>(v, t, sm);
+        if (!skip) xc_network<E, S::LK, S::LOGW>(v, t, sm, CtaBarrier{});
+        if (!skip || in != out) store_tile<E, S::K>(v, out + off, t * S::K, n);
+        __syncthreads();  // the next array's first layout change reuses the region
+    }
+}
+
+// k_sort_idlist with the transposed network (one array per CTA): the arrays
+// ids[0 .. count) of a CSR batch, count and list position read on the device
+// when d_count is set, CTAs pulling arrays from the queue at d_head when set.
+template <class E, class S, int MINB = 1>
+__global__ void __launch_bounds__(S::TPA, MINB)
+    k_sort_idlist_xc(const typename E::Mem* in, typename E::Mem* out, const int* __restrict__ off,
+                     const int* __restrict__ ids, int count, const int* d_count, const int* d_base, int* d_head) {
+    using R = typename E::Reg;
+    static_assert(S::LW > 0, "one array per CTA");
+    __shared__ int s_next;
+    if (d_count) {
+        count = *d_count;
+        ids += *d_base;
+    }
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* sm = reinterpret_cast<R*>(smem_raw);
+    const int t = int(threadIdx.x);
+    long long g = blockIdx.x;
+    for (;;) {
+        if (d_head) {
+            if (t == 0) s_next = atomicAdd(d_head, 1);
+            __syncthreads();
+            g = s_next;
+            __syncthreads();
+        }
+        if (g >= count) break;  // uniform across the CTA
+        const int a = ids[g];
+        const long long start = off[a];
+        const int na = off[a + 1] - off[a];
+        R v[S::K];
+        load_tile<E, S::K>(v, in + start, t * S::K, na);
+        xc_network<E, S::LK, S::LOGW>(v, t, sm, CtaBarrier{});
+        store_tile<E, S::K>(v, out + start, t * S::K, na);
         __syncthreads();
+        if (!d_head) g += gridDim.x;
     }
 }
 
@@ -219,7 +283,7 @@ __device__ __forceinline__ void xc_cluster_network(typename E::Reg (&v)[1 << LK]
 // padding cannot skip layers as in network.cuh's compact form).
 template <class E, int LK, int LT, int LC, int MINB = 1>
 __global__ void __launch_bounds__(1 << LT, MINB)
-    k_sort_cluster_xp(const typename E::Mem* in, typename E::Mem* out, int n, long long arrays, const int* off,
+    k_sort_cluster_xc(const typename E::Mem* in, typename E::Mem* out, int n, long long arrays, const int* off,
                       const int* ids, const int* d_count) {
     using R = typename E::Reg;
     namespace cg = cooperative_groups;

@@ -237,7 +237,7 @@ struct ElemRecI32S {
 };
 
 // ---- records: uint64 key + int32 payload -------------------------------------
-struct RegRecU64 {
+struct alignas(16) RegRecU64 {
     uint64_t key;
     int32_t data;
 };
@@ -273,7 +273,7 @@ struct ElemRecU64 {
     }
 };
 
-struct RegRecU64S {
+struct alignas(16) RegRecU64S {
     uint64_t key;
     int32_t data;
     int32_t pos;
@@ -317,5 +317,33 @@ struct ElemRecU64S {
 };
 
 // uint64 keys alone are totally ordered values: the stable mode changes nothing.
+
+// Shared-memory (and distributed-shared-memory) element accesses.  The
+// 16-byte register records move as one 128-bit access: field by field (an
+// 8-byte key, then a 4-byte payload at a 16-byte stride) each access takes
+// two wavefronts per half-warp instead of one per quarter-warp.
+template <class R>
+__device__ __forceinline__ R sh_ld(const R* p) {
+    return *p;
+}
+template <class R>
+__device__ __forceinline__ void sh_st(R* p, const R& v) {
+    *p = v;
+}
+__device__ __forceinline__ RegRecU64 sh_ld(const RegRecU64* p) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    return RegRecU64{(uint64_t(u.y) << 32) | u.x, int32_t(u.z)};
+}
+__device__ __forceinline__ void sh_st(RegRecU64* p, const RegRecU64& v) {
+    *reinterpret_cast<uint4*>(p) = make_uint4(unsigned(v.key), unsigned(v.key >> 32), unsigned(v.data), 0u);
+}
+__device__ __forceinline__ RegRecU64S sh_ld(const RegRecU64S* p) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    return RegRecU64S{(uint64_t(u.y) << 32) | u.x, int32_t(u.z), int32_t(u.w)};
+}
+__device__ __forceinline__ void sh_st(RegRecU64S* p, const RegRecU64S& v) {
+    *reinterpret_cast<uint4*>(p) =
+        make_uint4(unsigned(v.key), unsigned(v.key >> 32), unsigned(v.data), unsigned(v.pos));
+}
 
 }  // namespace b200s

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <type_traits>
 
 #include "cluster.cuh"
 #include "network.cuh"
@@ -120,13 +121,56 @@ struct Packed {
     }
 };
 
+// Opt in to SMEM bytes of dynamic shared memory for kernel fn (once per
+// device), with a margin for the kernel's own static variables.
+template <size_t SMEM>
+cudaError_t opt_in_smem(const void* fn, std::atomic<unsigned long long>& done) {
+    if (SMEM + 1024 <= 48 * 1024) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM));
+    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
+
+// CTAs of kernel fn resident at once on the current device (cached per device
+// in cache[]).
+inline cudaError_t resident_ctas(const void* fn, int cta, size_t smem, std::atomic<int>* cache, int* out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    int cap = cache[dev & 63].load(std::memory_order_relaxed);
+    if (cap == 0) {
+        int per_sm = 0, sms = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, cta, smem)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        cap = per_sm * sms;
+        if (cap <= 0) return cudaErrorInvalidConfiguration;
+        cache[dev & 63].store(cap, std::memory_order_relaxed);
+    }
+    *out = cap;
+    return cudaSuccess;
+}
+
 // A cluster of 2^LC CTAs per array (SB: single-buffered shared memory).
-template <class E, int LK, int LG, int LW, int LC, bool SB, int MINB = 1>
+// KERNEL: the kernel template with k_sort_cluster's parameters and
+// arguments; SMEM_ELEMS its shared-memory elements per CTA (0: SB ? W : 2W).
+// Launch form 3 (instantiate_xc.cuh) reuses this with the transposed network.
+template <class E, int LK, int LG, int LW, int LC, bool SB, int MINB = 1, class KERNEL = void,
+          size_t SMEM_ELEMS = 0>
 struct ClusterTile {
     using S = Shape<LK, LG, LW>;
     static constexpr int CTA = S::TPA;
     static constexpr int C = 1 << LC;
-    static constexpr size_t SMEM = (SB ? 1 : 2) * size_t(S::W) * sizeof(typename E::Reg);
+    static constexpr size_t SMEM = SMEM_ELEMS ? SMEM_ELEMS * sizeof(typename E::Reg)
+                                              : (SB ? 1 : 2) * size_t(S::W) * sizeof(typename E::Reg);
+    static constexpr auto kernel() {
+        if constexpr (std::is_void_v<KERNEL>) return k_sort_cluster<E, S, LC, SB, MINB>;
+        else return KERNEL::template fn<E, LK, LG + LW, LC, MINB>();
+    }
 
     static cudaLaunchConfig_t config(long long clusters, cudaStream_t st, cudaLaunchAttribute* attr) {
         cudaLaunchConfig_t cfg = {};
@@ -150,7 +194,7 @@ struct ClusterTile {
         if (e != cudaSuccess) return e;
         int v = cache[dev & 63].load(std::memory_order_relaxed);
         if (v == 0) {
-            auto fn = k_sort_cluster<E, S, LC, SB, MINB>;
+            auto fn = kernel();
             e = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      int(SMEM));
             if (e != cudaSuccess) return e;
@@ -173,7 +217,7 @@ struct ClusterTile {
         if (clusters < 1) clusters = 1;
         cudaLaunchAttribute attr;
         cudaLaunchConfig_t cfg = config(clusters, st, &attr);
-        return cudaLaunchKernelEx(&cfg, k_sort_cluster<E, S, LC, SB, MINB>, static_cast<const typename E::Mem*>(in),
+        return cudaLaunchKernelEx(&cfg, kernel(), static_cast<const typename E::Mem*>(in),
                                   static_cast<typename E::Mem*>(out), n, arrays, off, ids, d_count);
     }
     static cudaError_t launch(const void* in, void* out, int n, long long arrays, long long, cudaStream_t st,
@@ -189,7 +233,7 @@ struct ClusterTile {
         return run(in, out, 0, max_count, off, ids, d_count, max_count, st);
     }
     static cudaError_t attrs(cudaFuncAttributes* a) {
-        return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(k_sort_cluster<E, S, LC, SB, MINB>));
+        return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(kernel()));
     }
     static KernelEntry entry(int dtype) {
         return KernelEntry{dtype, E::kStable ? 1 : 0, LK, LG, LW, CTA, S::LOGW + LC, SMEM, 1, &launch, &attrs,

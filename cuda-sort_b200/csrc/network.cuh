@@ -149,12 +149,12 @@ __device__ __forceinline__ void layer(typename E::Reg (&v)[S::K], const int t,
         // both the publish and the partner read are bank-conflict free.
         sfor<0, S::K>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            cur[q * S::TPA + t] = v[q];
+            sh_st(&cur[q * S::TPA + t], v[q]);
         });
         bar();
         sfor<0, S::K>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            const R b = cur[(q ^ int(RM)) * S::TPA + (t ^ int(TM))];
+            const R b = sh_ld(&cur[(q ^ int(RM)) * S::TPA + (t ^ int(TM))]);
             v[q] = E::pick(v[q], b, upper);
         });
         if constexpr (single_buffer<Bar>::value) {
@@ -218,14 +218,14 @@ __device__ __forceinline__ void warp_layer_rt(typename E::Reg (&v)[S::K], const 
     using R = typename E::Reg;
     sfor<0, S::K>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
-        cur[q * S::TPA + t] = v[q];
+        sh_st(&cur[q * S::TPA + t], v[q]);
     });
     if constexpr (UA) bar.unaligned();
     else bar();
     if constexpr (LIVE) {
         sfor<0, S::K>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            const R b = cur[(q ^ int(RM)) * S::TPA + (t ^ tm)];
+            const R b = sh_ld(&cur[(q ^ int(RM)) * S::TPA + (t ^ tm)]);
             v[q] = E::pick(v[q], b, upper);
         });
     }

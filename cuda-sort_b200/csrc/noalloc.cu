@@ -32,7 +32,8 @@ b200s_status cuda_error(cudaError_t e, const char* what);
 int effective_stable(int dtype, uint32_t flags);
 unsigned ragged_family_mask(int dtype, int stable);
 unsigned ragged_dedicated_mask(int dtype, int stable);
-void dedicated_entries(int dtype, int stable, int nb, unsigned* mask, int* idx);
+void dedicated_entries(int dtype, int stable, int nb, unsigned* mask, int* idx, bool* xc);
+bool cluster_xc(int dtype, int stable, int entry);
 int lookup_default_entry(int dtype, int stable, long long n, int* persistent);
 
 namespace {
@@ -136,7 +137,8 @@ extern "C" b200s_status b200s_sort_ragged_noalloc(b200s_dtype dtype, uint32_t fl
     (void)lookup_default_entry(dtype, stable, 1, &unused_form);
     unsigned dedicated = ragged_dedicated_mask(dtype, stable);
     int dedicated_idx[kMaxBuckets] = {};
-    dedicated_entries(dtype, stable, rk->nb, &dedicated, dedicated_idx);
+    bool dedicated_xc[kMaxBuckets] = {};
+    dedicated_entries(dtype, stable, rk->nb, &dedicated, dedicated_idx, dedicated_xc);
     if (dedicated != (1u << rk->nb) - 1u) {
         e = rk->launch(d_in, d_out, d_offsets, s->ids, &s->ctl, ragged_family_mask(dtype, stable), dedicated,
                        sms * per_sm, cs);
@@ -145,14 +147,14 @@ extern "C" b200s_status b200s_sort_ragged_noalloc(b200s_dtype dtype, uint32_t fl
     for (int b = rk->nb - 1; b >= 0; --b) {
         if (!((dedicated >> b) & 1u)) continue;
         const KernelEntry& k = registry()[size_t(dedicated_idx[b])];
-        e = k.launch_list_dev(d_in, d_out, d_offsets, s->ids, &s->ctl.count[b], &s->ctl.base[b], &s->ctl.dhead[b], n,
-                              cs);
+        e = (dedicated_xc[b] ? k.launch_list_dev_xc : k.launch_list_dev)(
+            d_in, d_out, d_offsets, s->ids, &s->ctl.count[b], &s->ctl.base[b], &s->ctl.dhead[b], n, cs);
         if (e != cudaSuccess) return cuda_error(e, "dedicated bucket launch");
     }
     for (int i = 0; i < spec.n_over; ++i) {
         const KernelEntry& k = registry()[size_t(cluster_idx[i])];
-        e = k.launch_cluster_list(d_in, d_out, d_offsets, s->oids + size_t(i) * kNoAllocArrays, &s->ctl.ocount[i],
-                                  n, cs);
+        e = (cluster_xc(dtype, stable, cluster_idx[i]) ? k.launch_cluster_list_xc : k.launch_cluster_list)(
+            d_in, d_out, d_offsets, s->oids + size_t(i) * kNoAllocArrays, &s->ctl.ocount[i], n, cs);
         if (e != cudaSuccess) return cuda_error(e, "cluster bucket launch");
     }
     return B200S_OK;

@@ -74,18 +74,32 @@ unsigned ragged_dedicated_mask(int dtype, int stable) {
 // 2^(kRaggedLmin + b)): the tabled single-CTA tile of that working length.
 // Buckets without one (none tabled, or a cluster tile) stay in the persistent
 // kernel: their bit is cleared in *mask.  idx[b] receives the entry.
-void dedicated_entries(int dtype, int stable, int nb, unsigned* mask, int* idx) {
+// xc[b] (optional): the table's launch form for that length is 3 and the
+// tile has the transposed-network form.
+void dedicated_entries(int dtype, int stable, int nb, unsigned* mask, int* idx, bool* xc) {
     for (int b = 0; b < nb; ++b) {
         idx[b] = -1;
+        if (xc) xc[b] = false;
         if (!((*mask >> b) & 1u)) continue;
         int persistent = 0;
         const int e = lookup_default_entry(dtype, stable, 1LL << (kRaggedLmin + b), &persistent);
         if (e >= 0 && registry()[size_t(e)].lc < 0 && registry()[size_t(e)].launch_list_dev &&
-            registry()[size_t(e)].log2w == kRaggedLmin + b)
+            registry()[size_t(e)].log2w == kRaggedLmin + b) {
             idx[b] = e;
-        else
+            if (xc) xc[b] = persistent == 3 && registry()[size_t(e)].launch_list_dev_xc;
+        } else {
             *mask &= ~(1u << b);
+        }
     }
+}
+
+// Whether the cluster tile `entry` runs its transposed-network form: the
+// table's launch form for its working length is 3 and the form is compiled.
+bool cluster_xc(int dtype, int stable, int entry) {
+    const KernelEntry& k = registry()[size_t(entry)];
+    if (!k.launch_cluster_list_xc) return false;
+    int form = 0;
+    return lookup_default_entry(dtype, stable, 1LL << k.log2w, &form) >= 0 && form == 3;
 }
 
 }  // namespace b200s
@@ -102,6 +116,7 @@ struct b200s_plan {
     unsigned family_mask = 0;
     unsigned dedicated_mask = 0;         // buckets with their own launch
     int dedicated_entry[kMaxBuckets] = {};
+    bool dedicated_xc[kMaxBuckets] = {};  // run the tile's transposed-network form
     int grid = 0;       // persistent CTAs
     int bin_grid = 0;   // CTAs of the binning kernels
     void* scratch = nullptr;
@@ -110,6 +125,7 @@ struct b200s_plan {
     int* oids = nullptr;          // cluster-bucket id lists, stride max_arrays
     BinSpec spec = {};
     int over_entry[kMaxOverflow] = {};  // registry index of each cluster bucket
+    bool over_xc[kMaxOverflow] = {};
     static constexpr int kSides = 4;
     cudaStream_t capture = nullptr;
     cudaStream_t side[kSides] = {};  // cluster and dedicated buckets run beside the persistent kernel
@@ -163,8 +179,8 @@ b200s_status record_sequence(b200s_plan* p, const void* in, void* out, const int
         const KernelEntry& ke = registry()[size_t(p->over_entry[i])];
         cudaStream_t ss = side_stream(k++);
         if (!ss) return cuda_error(e, "fork");
-        e = ke.launch_cluster_list(in, out, off, p->oids + size_t(i) * p->spec.stride, &p->ctl->ocount[i],
-                                   max_count, ss);
+        e = (p->over_xc[i] ? ke.launch_cluster_list_xc : ke.launch_cluster_list)(
+            in, out, off, p->oids + size_t(i) * p->spec.stride, &p->ctl->ocount[i], max_count, ss);
         if (e != cudaSuccess) return cuda_error(e, "cluster bucket launch");
     }
     for (int b = p->spec.nb - 1; b >= 0; --b) {
@@ -172,8 +188,8 @@ b200s_status record_sequence(b200s_plan* p, const void* in, void* out, const int
         const KernelEntry& ke = registry()[size_t(p->dedicated_entry[b])];
         cudaStream_t ss = side_stream(k++);
         if (!ss) return cuda_error(e, "fork");
-        e = ke.launch_list_dev(in, out, off, p->ids, &p->ctl->count[b], &p->ctl->base[b], &p->ctl->dhead[b],
-                               max_count, ss);
+        e = (p->dedicated_xc[b] ? ke.launch_list_dev_xc : ke.launch_list_dev)(
+            in, out, off, p->ids, &p->ctl->count[b], &p->ctl->base[b], &p->ctl->dhead[b], max_count, ss);
         if (e != cudaSuccess) return cuda_error(e, "dedicated bucket launch");
     }
     const uint32_t all = (1u << p->spec.nb) - 1u;
@@ -257,13 +273,14 @@ b200s_status b200s_plan_create(b200s_plan** out, b200s_dtype dtype, uint32_t fla
     (void)lookup_default_entry(dtype, stable, 1, &unused_form);
     p->family_mask = ragged_family_mask(dtype, stable);
     p->dedicated_mask = ragged_dedicated_mask(dtype, stable);
-    dedicated_entries(dtype, stable, rk->nb, &p->dedicated_mask, p->dedicated_entry);
+    dedicated_entries(dtype, stable, rk->nb, &p->dedicated_mask, p->dedicated_entry, p->dedicated_xc);
     p->grid = sms * per_sm;
     p->bin_grid = sms * 4;
     const long long stride = std::max<long long>(1, max_arrays);
     p->spec.nb = rk->nb;
     p->spec.over_lo = kRaggedLmin + rk->nb;
     p->spec.n_over = overflow_entries(dtype, stable, p->spec.over_lo, p->over_entry);
+    for (int i = 0; i < p->spec.n_over; ++i) p->over_xc[i] = cluster_xc(dtype, stable, p->over_entry[i]);
     p->spec.stride = int(stride);
     // control block, bucketed ids, plain ids, cluster-bucket ids
     const size_t ids_bytes = size_t(stride) * sizeof(int);
@@ -459,7 +476,8 @@ b200s_status b200s_sort_ragged_plain(b200s_plan* p, const void* d_in, void* d_ou
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     for (const auto& g : p->groups) {
         const KernelEntry& k = registry()[size_t(g.entry)];
-        e = k.launch_list(d_in, d_out, d_offsets, p->plain_ids + g.first, g.count, st);
+        e = (g.persistent == 3 && k.launch_list_xc ? k.launch_list_xc : k.launch_list)(
+            d_in, d_out, d_offsets, p->plain_ids + g.first, g.count, st);
         if (e != cudaSuccess) return cuda_error(e, "per-length launch");
     }
     return B200S_OK;

@@ -43,6 +43,16 @@ struct KernelEntry {
     cudaError_t (*launch_cluster_list)(const void* in, void* out, const int* d_off, const int* d_ids,
                                        const int* d_count, int max_count, cudaStream_t stream);
     ListLaunchDev launch_list_dev;  // single-CTA tiles only (null for cluster kernels)
+    // Launch form 3 of a multi-warp or cluster tile: the same tile running the
+    // transposed network of cta_xpose.cuh (null where none is compiled).
+    // Packed batch, host-counted id list, device-counted id list (single-CTA
+    // tiles) and cluster id list with a device count (cluster tiles).
+    PackedLaunch launch_xc = nullptr;
+    ListLaunch launch_list_xc = nullptr;
+    ListLaunchDev launch_list_dev_xc = nullptr;
+    cudaError_t (*launch_cluster_list_xc)(const void* in, void* out, const int* d_off, const int* d_ids,
+                                          const int* d_count, int max_count, cudaStream_t stream) = nullptr;
+    size_t smem_xc = 0;  // its dynamic shared memory bytes
 };
 
 void register_i32(std::vector<KernelEntry>& out);
@@ -51,6 +61,12 @@ void register_u64(std::vector<KernelEntry>& out);
 void register_cluster_keys(std::vector<KernelEntry>& out);
 void register_cluster_rec(std::vector<KernelEntry>& out);
 void register_cluster_u64rec(std::vector<KernelEntry>& out);
+// Launch form 3 of multi-warp and cluster tiles, attached to the entries
+// above (run last).
+void register_xc_keys(std::vector<KernelEntry>& out);
+void register_xc_rec(std::vector<KernelEntry>& out);
+void register_xc_cluster_rec(std::vector<KernelEntry>& out);
+void register_xc_u64rec(std::vector<KernelEntry>& out);
 
 const std::vector<KernelEntry>& registry();
 

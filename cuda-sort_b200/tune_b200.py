@@ -4,10 +4,10 @@ at first use from beside libb200sort.so).
   python cuda-sort_b200/tune_b200.py [--out PATH] [--summary PATH] [--passes P]
 
 For every element type, stable flag and working length W = 2^L it times each
-compiled single-CTA tile of that W in each launch form it has (0 one slot per
-array, 1 persistent with register prefetch, 2 persistent TMA pipeline, 3
-transposed network) on a full-length batch of about 4 M elements, checks the
-output, and keeps the fastest as the packed row.  For the ragged kernel it
+compiled tile of that W (single-CTA and cluster tiles) in each launch form it
+has (0 one slot per array, 1 persistent with register prefetch, 2 persistent
+TMA pipeline, 3 transposed network) on a full-length batch of about 4 M
+elements, checks the output, and keeps the fastest as the packed row.  For the ragged kernel it
 times, per bucket L, a batch whose lengths all fall in that bucket in the
 persistent kernel with the bucket's shape family A, with family B, and as a
 launch of its own (the tabled tile of its working length, beside the
@@ -48,7 +48,7 @@ def _keys(dtype, arr):
 
 def tune_packed(dtype, flags, flush, passes, log, summary):
     rows = []
-    tiles = [t for t in bs.tiles(dtype, flags) if t.log2_ctas == 0 and t.cta_threads > 0]
+    tiles = [t for t in bs.tiles(dtype, flags) if t.cta_threads > 0]   # single-CTA and cluster tiles
     by_w = {}
     for t in tiles:
         by_w.setdefault(sum(t.as_tuple()), []).append(t)
@@ -65,7 +65,9 @@ def tune_packed(dtype, flags, flush, passes, log, summary):
         cands = []
         for base in by_w[L]:
             info = bs.tile_info(dtype, n, flags, base)
-            forms = [0, 1] + ([2] if info.tma_form else []) + ([3] if info.xpose_form else [])
+            # cluster tiles (no arrays per CTA) have one launch besides form 3
+            forms = ([0] if info.arrays_per_cta == 0 else [0, 1]) + ([2] if info.tma_form else []) + \
+                ([3] if info.xpose_form else [])
             cands += [base.with_form(f) for f in forms]
         results = []
         for tile in cands:
@@ -83,18 +85,26 @@ def tune_packed(dtype, flags, flush, passes, log, summary):
         (us, spread, t) = results[0]
         second = results[1] if len(results) > 1 else None
         tail = (", runner-up %.2f us %s" % (second[0], _shape(second[2]))) if second else ""
-        rows.append("%d,%d,%d,%d,%d,%d,%d  # %.2f us (spread %.1f %%)%s, %d arrays"
-                    % (dtype, flags, L, t.log2_items, t.log2_lanes, t.log2_warps, t.persistent, us, 100 * spread, tail,
-                       arrays))
+        lc = (",%d" % t.log2_ctas) if t.log2_ctas else ""
+        rows.append("%d,%d,%d,%d,%d,%d,%d%s  # %.2f us (spread %.1f %%)%s, %d arrays"
+                    % (dtype, flags, L, t.log2_items, t.log2_lanes, t.log2_warps, t.persistent, lc, us, 100 * spread,
+                       tail, arrays))
         summary.append(("packed", dtype, flags, n, arrays, _shape(t), us, spread,
                         _shape(second[2]) if second else "-", second[0] if second else None))
         del ins, outs, src
         torch.cuda.empty_cache()
+    # the ragged rows are timed with these packed rows in force (a launch of
+    # its own runs the tabled tile in its tabled form)
+    with tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False) as f:
+        f.write("\n".join(r.split("#")[0] for r in rows) + "\n")
+    bs.load_tile_table(f.name)
+    os.unlink(f.name)
     return rows
 
 
 def _shape(t):
-    return "K%d.G%d.W%d/%s" % (1 << t.log2_items, 1 << t.log2_lanes, 1 << t.log2_warps, FORM_NAMES[t.persistent])
+    c = ".C%d" % (1 << t.log2_ctas) if t.log2_ctas else ""
+    return "K%d.G%d.W%d%s/%s" % (1 << t.log2_items, 1 << t.log2_lanes, 1 << t.log2_warps, c, FORM_NAMES[t.persistent])
 
 
 def tune_ragged(dtype, flags, flush, passes, log, summary):

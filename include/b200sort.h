@@ -96,7 +96,8 @@ typedef struct b200s_tile {
                             comparator layer in registers with the tile re-laid out through
                             shared memory between register windows (single-warp tiles of
                             int32 and uint64 keys, IntAndData records and stable records up
-                            to W = 1024, with element-aligned buffers; b200s_tile_info's
+                            to W = 1024, with element-aligned buffers; and the multi-warp
+                            and cluster tiles of every element type; b200s_tile_info's
                             xpose_form tells which; form 0 otherwise) */
     int32_t log2_ctas;   /* CTAs per array: 0 for single-CTA tiles (cluster tiles of one
                             CTA exist only where no single-CTA tile of that shape does) */
@@ -144,7 +145,8 @@ b200s_status b200s_tma_timeouts(int64_t* count);
 b200s_status b200s_test_stall_tma_loads(int32_t enable);
 /* Replace rows of the default tile table from a CSV file; '#' starts a
  * comment.  Packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps
- * [,form] (form: 0 .. 3 as b200s_tile.persistent).  Ragged rows: r,dtype,flags,log2_w,family (0: the
+ * [,form[,log2_ctas]] (form: 0 .. 3 as b200s_tile.persistent; log2_ctas: CTAs
+ * per array of a cluster tile, default 0).  Ragged rows: r,dtype,flags,log2_w,family (0: the
  * persistent kernel with the larger per-thread tile, 1: with the smaller one, 2: a launch of its own of the
  * packed table's tile for that length), read by plans created afterwards.
  * Returns the number of rows applied in *applied. */
