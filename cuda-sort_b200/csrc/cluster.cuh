@@ -47,7 +47,7 @@ __device__ __forceinline__ void cluster_layer(typename E::Reg (&v)[S::K], const 
         const R* remote = cluster.map_shared_rank(cur, int(unsigned(rank) ^ CM));
         sfor<0, S::K>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            const R b = sh_ld(&remote[(q ^ int(RM)) * S::TPA + (t ^ int(TM))]);
+            const R b = dsm_ld(&remote[(q ^ int(RM)) * S::TPA + (t ^ int(TM))]);
             v[q] = E::pick(v[q], b, upper);
         });
         cluster.sync();
@@ -81,7 +81,7 @@ __device__ __forceinline__ void cta_layer_rt(typename E::Reg (&v)[S::K], const i
         const R* remote = cluster.map_shared_rank(cur, rank ^ cm);
         sfor<0, S::K>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            const R b = sh_ld(&remote[(q ^ int(RM)) * S::TPA + (t ^ int(TM))]);
+            const R b = dsm_ld(&remote[(q ^ int(RM)) * S::TPA + (t ^ int(TM))]);
             v[q] = E::pick(v[q], b, upper);
         });
     }

@@ -160,7 +160,12 @@ __device__ __forceinline__ void xc_stage(typename E::Reg (&v)[1 << LK], const in
 template <class E, int LK, int LOGW, class Bar>
 __device__ __forceinline__ void xc_network(typename E::Reg (&v)[1 << LK], const int t, typename E::Reg* sm,
                                            const Bar& bar) {
-    sfor<0, LOGW>([&](auto sc) { xc_stage<E, LK, decltype(sc)::value>(v, t, sm, bar); });
+    if constexpr (keys_only<E>::value) {
+        xp_reg_sort_oem<E, LK>(v);  // keys alone: stages 0 .. LK-1 with fewer comparators
+        sfor<LK, LOGW>([&](auto sc) { xc_stage<E, LK, decltype(sc)::value>(v, t, sm, bar); });
+    } else {
+        sfor<0, LOGW>([&](auto sc) { xc_stage<E, LK, decltype(sc)::value>(v, t, sm, bar); });
+    }
 }
 
 // Shared-memory elements of a slice of 2^LOGW elements in this layout.
@@ -187,7 +192,7 @@ __device__ __forceinline__ void xc_cluster_layer(typename E::Reg (&v)[1 << LK], 
     const int pb = xp_addr<LK>(REFLECT ? T - 1 - t : t);
     sfor<0, K>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
-        const R b = sh_ld(&remote[pb + xp_addr<LK>((REFLECT ? K - 1 - q : q) << LT)]);
+        const R b = dsm_ld(&remote[pb + xp_addr<LK>((REFLECT ? K - 1 - q : q) << LT)]);
         v[q] = E::pick(v[q], b, upper);
     });
     cluster.sync();

@@ -102,6 +102,7 @@ __device__ __forceinline__ uint64_t shfl_d(uint64_t v, int d) {
 
 // ---- int32 keys --------------------------------------------------------------
 struct ElemI32 {
+    static constexpr bool kKeysOnly = true;  // tie order unobservable
     using Mem = int32_t;
     using Reg = int32_t;
     static constexpr bool kStable = false;
@@ -137,6 +138,7 @@ struct ElemI32C : ElemI32 {
 
 // ---- uint64 keys -------------------------------------------------------------
 struct ElemU64 {
+    static constexpr bool kKeysOnly = true;
     using Mem = uint64_t;
     using Reg = uint64_t;
     static constexpr bool kStable = false;
@@ -330,12 +332,32 @@ template <class R>
 __device__ __forceinline__ void sh_st(R* p, const R& v) {
     *p = v;
 }
+// The fourth word is padding: one 128-bit shared-space load in PTX (p is in
+// this CTA's shared memory), so that the compiler does not narrow it to an
+// 8-byte and a 4-byte load.
 __device__ __forceinline__ RegRecU64 sh_ld(const RegRecU64* p) {
-    const uint4 u = *reinterpret_cast<const uint4*>(p);
-    return RegRecU64{(uint64_t(u.y) << 32) | u.x, int32_t(u.z)};
+    unsigned x, y, z, w;
+    const unsigned a = unsigned(__cvta_generic_to_shared(p));
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(x), "=r"(y), "=r"(z), "=r"(w) : "r"(a) : "memory");
+    (void)w;
+    return RegRecU64{(uint64_t(y) << 32) | x, int32_t(z)};
 }
 __device__ __forceinline__ void sh_st(RegRecU64* p, const RegRecU64& v) {
     *reinterpret_cast<uint4*>(p) = make_uint4(unsigned(v.key), unsigned(v.key >> 32), unsigned(v.data), 0u);
+}
+// Reads of a cluster peer's shared memory (a generic pointer from
+// map_shared_rank): plain loads, 128 bits for the 16-byte records.
+template <class R>
+__device__ __forceinline__ R dsm_ld(const R* p) {
+    return *p;
+}
+__device__ __forceinline__ RegRecU64 dsm_ld(const RegRecU64* p) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    return RegRecU64{(uint64_t(u.y) << 32) | u.x, int32_t(u.z)};
+}
+__device__ __forceinline__ RegRecU64S dsm_ld(const RegRecU64S* p) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    return RegRecU64S{(uint64_t(u.y) << 32) | u.x, int32_t(u.z), int32_t(u.w)};
 }
 __device__ __forceinline__ RegRecU64S sh_ld(const RegRecU64S* p) {
     const uint4 u = *reinterpret_cast<const uint4*>(p);

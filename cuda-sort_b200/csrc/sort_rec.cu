@@ -29,6 +29,10 @@ void register_rec(std::vector<KernelEntry>& o) {
     o.push_back(Packed<ElemRecI32, 5, 4, 0>::entry(1));
     o.push_back(Packed<ElemRecI32, 5, 5, 0>::entry(1));
     o.push_back(Packed<ElemRecI32, 5, 5, 1>::entry(1));
+    // 32 records per thread for W = 4096 and 8192 (128 and 256 threads): the
+    // transposed form needs fewer window moves than with 16 per thread.
+    o.push_back(Packed<ElemRecI32, 5, 5, 2, true>::entry(1));
+    o.push_back(Packed<ElemRecI32, 5, 5, 3, true>::entry(1));
 }
 
 }  // namespace b200s

@@ -12,6 +12,8 @@ void register_xc_rec(std::vector<KernelEntry>& o) {
     PackedXc<ElemRecI32, 4, 3, 4>::attach_to(o, 1);
     PackedXc<ElemRecI32, 4, 4, 2>::attach_to(o, 1);   // W = 8192
     PackedXc<ElemRecI32, 5, 1, 8>::attach_to(o, 1);   // W = 2048, 32 records per thread
+    PackedXc<ElemRecI32, 5, 2, 4>::attach_to(o, 1);   // W = 4096
+    PackedXc<ElemRecI32, 5, 3, 2>::attach_to(o, 1);   // W = 8192
     PackedXc<ElemRecI32S, 4, 1, 8>::attach_to(o, 1);
     PackedXc<ElemRecI32S, 4, 2, 4>::attach_to(o, 1);
     PackedXc<ElemRecI32S, 4, 3, 2>::attach_to(o, 1);

@@ -85,6 +85,61 @@ __device__ __forceinline__ void xp_stcs(uint64_t* p, uint64_t v) {
 }
 __device__ __forceinline__ void xp_stcs(RecI32* p, RecI32 v) { __stcs(reinterpret_cast<int2*>(p), make_int2(v.key, v.data)); }
 
+// Element types whose tie order cannot be observed (keys alone: equal keys
+// are indistinguishable) may sort a thread's registers with any network that
+// leaves them in ascending order; records keep the reflection network.
+template <class E, class = void>
+struct keys_only : std::false_type {};
+template <class E>
+struct keys_only<E, std::void_t<decltype(E::kKeysOnly)>> : std::integral_constant<bool, E::kKeysOnly> {};
+
+// Batcher's odd-even merge sort of N = 2^L registers, in its published
+// iterative form (for p = 1, 2, 4, ...; k = p, p/2, ..., 1; j = k mod p,
+// j + 2k, ...; i < k: compare j+i with j+i+k when both lie in the same block
+// of 2p): the lower index receives the minimum.  Same depth as the bitonic
+// sort, fewer comparators (191 instead of 240 for 32 registers, 63 instead of
+// 80 for 16), and the same result for keys: the registers end sorted, as
+// after stages 0 .. L-1 of the reflection network.
+template <int N>
+struct OddEvenMergeSort {
+    struct Pair {
+        int a, b;
+    };
+    static constexpr int count() {
+        int c = 0;
+        for (int p = 1; p < N; p *= 2)
+            for (int k = p; k >= 1; k /= 2)
+                for (int j = k % p; j <= N - 1 - k; j += 2 * k)
+                    for (int i = 0; i <= k - 1 && i <= N - j - k - 1; ++i)
+                        if ((i + j) / (2 * p) == (i + j + k) / (2 * p)) ++c;
+        return c;
+    }
+    struct Table {
+        Pair pairs[count()];
+    };
+    static constexpr Table table() {
+        Table t{};
+        int c = 0;
+        for (int p = 1; p < N; p *= 2)
+            for (int k = p; k >= 1; k /= 2)
+                for (int j = k % p; j <= N - 1 - k; j += 2 * k)
+                    for (int i = 0; i <= k - 1 && i <= N - j - k - 1; ++i)
+                        if ((i + j) / (2 * p) == (i + j + k) / (2 * p)) t.pairs[c++] = Pair{i + j, i + j + k};
+        return t;
+    }
+    static constexpr Table kTable = table();
+};
+
+template <class E, int LK>
+__device__ __forceinline__ void xp_reg_sort_oem(typename E::Reg (&v)[1 << LK]) {
+    using T = OddEvenMergeSort<(1 << LK)>;
+    sfor<0, T::count()>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        constexpr int a = T::kTable.pairs[i].a, b = T::kTable.pairs[i].b;
+        xcex<E, i>(v[a], v[b]);
+    });
+}
+
 template <int LK>
 __host__ __device__ constexpr int xp_addr(int i) {
     return i + (i >> LK);
@@ -191,13 +246,18 @@ template <class E, int LK, int LG>
 __device__ __forceinline__ void xp_network(typename E::Reg (&v)[1 << LK], const int t, typename E::Reg* sm,
                                            const bool check = false) {
     bool done = false;
-    sfor<0, LK>([&](auto sc) {
-        constexpr int ST = decltype(sc)::value;
-        if (!done) {
-            xp_reg_stage<E, LK, ST>(v);
-            if (ST >= 4 && check) done = xp_warp_in_order<E, LK, LG>(v, t);
-        }
-    });
+    if constexpr (keys_only<E>::value) {
+        xp_reg_sort_oem<E, LK>(v);  // stages 0 .. LK-1 with fewer comparators
+        if (LK >= 5 && check) done = xp_warp_in_order<E, LK, LG>(v, t);
+    } else {
+        sfor<0, LK>([&](auto sc) {
+            constexpr int ST = decltype(sc)::value;
+            if (!done) {
+                xp_reg_stage<E, LK, ST>(v);
+                if (ST >= 4 && check) done = xp_warp_in_order<E, LK, LG>(v, t);
+            }
+        });
+    }
     sfor<LK, LK + LG>([&](auto sc) {
         constexpr int ST = decltype(sc)::value;
         if (!done) {
