@@ -71,6 +71,15 @@ const std::vector<KernelEntry>& registry() {
         register_xc_rec(v);
         register_xc_cluster_rec(v);
         register_xc_u64rec(v);
+        // single-warp tiles: launch form 3 over id lists is the one-warp
+        // transposed network (xpose.cuh)
+        for (KernelEntry& k : v)
+            if (k.lw == 0 && k.lc < 0)
+                for (const XposeEntry& x : xpose_registry())
+                    if (x.dtype == k.dtype && x.stable == k.stable && x.lk == k.lk && x.lg == k.lg) {
+                        k.launch_list_xc = x.launch_list;
+                        k.launch_list_dev_xc = x.launch_list_dev;
+                    }
         return v;
     }();
     return all;

@@ -5,6 +5,7 @@
 // coalesced through the shared region, keeping their order (the reference's
 // tie order depends on it).  Both store coalesced through the shared region.
 #include <algorithm>
+#include <atomic>
 
 #include "xpose.cuh"
 #include "xpose_registry.h"
@@ -34,9 +35,42 @@ struct Xpose {
     static cudaError_t attrs(cudaFuncAttributes* a) {
         return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(kernel()));
     }
+    static constexpr auto list_kernel() { return k_sort_xpose_list<E, LK, LG, MINB, IO>; }
+    static cudaError_t launch_list(const void* in, void* out, const int* off, const int* ids, int count,
+                                   cudaStream_t st) {
+        const int grid = std::max(1, (count + APW - 1) / APW);
+        list_kernel()<<<dim3(unsigned(grid)), dim3(32), SMEM, st>>>(static_cast<const typename E::Mem*>(in),
+                                                                   static_cast<typename E::Mem*>(out), off, ids,
+                                                                   count, nullptr, nullptr, nullptr);
+        return cudaGetLastError();
+    }
+    // Resident warps (cached per device), at most what max_count arrays need,
+    // pulling arrays from the queue.
+    static cudaError_t launch_list_dev(const void* in, void* out, const int* off, const int* ids, const int* d_count,
+                                       const int* d_base, int* d_head, int max_count, cudaStream_t st) {
+        static std::atomic<int> resident[64];
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        int cap = resident[dev & 63].load(std::memory_order_relaxed);
+        if (cap == 0) {
+            int per_sm = 0, sms = 0;
+            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, list_kernel(), 32, SMEM)) != cudaSuccess)
+                return e;
+            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+            cap = per_sm * sms;
+            if (cap <= 0) return cudaErrorInvalidConfiguration;
+            resident[dev & 63].store(cap, std::memory_order_relaxed);
+        }
+        const int need = std::max(1, (max_count + APW - 1) / APW);
+        list_kernel()<<<dim3(unsigned(std::min(need, cap))), dim3(32), SMEM, st>>>(
+            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), off, ids, 0, d_count, d_base,
+            d_head);
+        return cudaGetLastError();
+    }
     static XposeEntry entry(int dtype) {
-        return XposeEntry{dtype, E::kStable ? 1 : 0, LK, LG, &launch, &attrs, WPC * 32, SMEM,
-                          int(sizeof(typename E::Mem))};
+        return XposeEntry{dtype,    E::kStable ? 1 : 0, LK,   LG, &launch, &attrs, WPC * 32, SMEM,
+                          int(sizeof(typename E::Mem)), &launch_list, &launch_list_dev};
     }
 };
 

@@ -419,4 +419,53 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
     }
 }
 
+// The same over a list of CSR arrays (a ragged plan's length class): arrays
+// ids[0 .. count) with array a at [off[a], off[a+1]); count and the list's
+// first position read on the device when d_count is set; each warp pulls
+// its next arrays from the queue at d_head when set (one atomicAdd per
+// warp), else strides over the list.
+template <class E, int LK, int LG, int MINB, int IO>
+__global__ void __launch_bounds__(32, MINB)
+    k_sort_xpose_list(const typename E::Mem* in, typename E::Mem* out, const int* __restrict__ off,
+                      const int* __restrict__ ids, int count, const int* d_count, const int* d_base, int* d_head) {
+    constexpr bool STRIPED = IO == kXpIoStriped;
+    using R = typename E::Reg;
+    constexpr int K = 1 << LK, G = 1 << LG, APW = 32 / G;
+    static_assert(LG <= 5 && LG <= LK && LG >= 1, "one warp or less per array, at most two windows");
+    static_assert(!STRIPED || !E::kStable, "striped access relabels the input: keys only");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = int(threadIdx.x) & 31;
+    const int slot = lane >> LG, t = lane & (G - 1);
+    R* sm = reinterpret_cast<R*>(smem_raw) + slot * xp_region<LK, LG>();
+    if (d_count) {
+        count = *d_count;
+        ids += *d_base;
+    }
+    long long first = (long long)blockIdx.x * APW;
+    for (;;) {
+        if (d_head) {
+            int f = 0;
+            if (lane == 0) f = atomicAdd(d_head, APW);
+            first = __shfl_sync(0xffffffffu, f, 0);
+        }
+        if (first >= count) break;  // uniform across the warp
+        const long long g = first + slot;
+        int na = 0;
+        long long start = 0;
+        if (g < count) {
+            const int a = ids[g];
+            start = off[a];
+            na = off[a + 1] - off[a];
+        }
+        R v[K];
+        if constexpr (IO == kXpIoStaged) xp_load_staged<E, LK, LG>(v, in + start, t, na, sm);
+        else if constexpr (STRIPED) xp_load_striped<E, LK, LG>(v, in + start, t, na);
+        else load_tile<E, K>(v, in + start, t * K, na);
+        xp_network<E, LK, LG>(v, t, sm, false);
+        if constexpr (IO != kXpIoBlocked) xp_store_striped<E, LK, LG>(v, out + start, t, na, sm);
+        else store_tile<E, K>(v, out + start, t * K, na);
+        if (!d_head) first += (long long)gridDim.x * APW;
+    }
+}
+
 }  // namespace b200s

@@ -17,6 +17,13 @@ struct XposeEntry {
     int cta;      // threads per CTA
     size_t smem;  // dynamic shared memory per CTA
     int align;    // the arrays' buffers must be aligned to this many bytes (one element)
+    // The same network over a CSR id list (a ragged length class): host count,
+    // or count and list position on the device with a work queue.
+    cudaError_t (*launch_list)(const void* in, void* out, const int* d_off, const int* d_ids, int count,
+                               cudaStream_t stream);
+    cudaError_t (*launch_list_dev)(const void* in, void* out, const int* d_off, const int* d_ids,
+                                   const int* d_count, const int* d_base, int* d_head, int max_count,
+                                   cudaStream_t stream);
 };
 
 const std::vector<XposeEntry>& xpose_registry();

@@ -86,14 +86,18 @@ def _restore():
 
 @pytest.mark.parametrize("dtype,flags", [(bs.I32_I32, 0), (bs.I32_I32, bs.STABLE), (bs.U64_I32, 0), (bs.U64, 0)])
 def test_ragged_plan_runs_form3_for_its_classes(dtype, flags):
-    # every multi-warp length class on a launch of its own with its form-3
-    # tile, and the cluster classes in form 3: graph, direct, hinted, plain per
-    # class and the allocation-free path all equal the oracle
+    # every length class with a form-3 tile (one-warp, multi-warp) on a launch
+    # of its own in that form, and the cluster classes in form 3: graph,
+    # direct, hinted, plain per class and the allocation-free path all equal
+    # the oracle
     import ctypes
     import torch
     top = bs.ragged_max_length(dtype, flags)
     rows = []
-    for tile in xc_tiles(dtype, flags):
+    one_warp = [b.with_form(3) for b in bs.tiles(dtype, flags)
+                if b.log2_warps == 0 and b.log2_ctas == 0 and b.log2_lanes > 0
+                and bs.tile_info(dtype, 1 << sum(b.as_tuple()), flags, b).xpose_form]
+    for tile in one_warp + xc_tiles(dtype, flags):
         w = width(tile)
         L = w.bit_length() - 1
         rows.append((dtype, flags, L) + tile.as_tuple()[:3] + (3, tile.log2_ctas))
