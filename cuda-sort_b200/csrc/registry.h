@@ -56,6 +56,7 @@ struct KernelEntry {
 };
 
 void register_i32(std::vector<KernelEntry>& out);
+void register_i32_alt(std::vector<KernelEntry>& out);  // called by register_i32
 void register_rec(std::vector<KernelEntry>& out);
 void register_u64(std::vector<KernelEntry>& out);
 void register_cluster_keys(std::vector<KernelEntry>& out);

@@ -17,18 +17,7 @@ void register_i32(std::vector<KernelEntry>& o) {
     o.push_back(Packed<ElemI32, 5, 5, 2>::entry(D));
     o.push_back(Packed<ElemI32, 5, 5, 3>::entry(D));
     o.push_back(Packed<ElemI32, 5, 5, 4>::entry(D));  // W = 16384, 512 threads
-    // K = 16 alternatives for the tile table.
-    o.push_back(Packed<ElemI32, 4, 1, 0>::entry(D));
-    o.push_back(Packed<ElemI32, 4, 2, 0>::entry(D));
-    o.push_back(Packed<ElemI32, 4, 3, 0>::entry(D));
-    o.push_back(Packed<ElemI32, 4, 4, 0>::entry(D));
-    o.push_back(Packed<ElemI32, 4, 5, 0>::entry(D));
-    o.push_back(Packed<ElemI32, 4, 5, 1>::entry(D));
-    o.push_back(Packed<ElemI32, 4, 5, 2>::entry(D));
-    // K = 64: ten shuffle layers instead of fifteen for a 1024-key array.
-    o.push_back(Packed<ElemI32, 6, 3, 0>::entry(D));
-    o.push_back(Packed<ElemI32, 6, 4, 0>::entry(D));
-    o.push_back(Packed<ElemI32, 6, 5, 0>::entry(D));
+    register_i32_alt(o);  // the alternatives, compiled in their own unit
 }
 
 }  // namespace b200s
