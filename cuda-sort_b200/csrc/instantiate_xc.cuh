@@ -92,6 +92,9 @@ struct ClusterXc {
                 k.launch_list_xc = &Tile::launch_list;
                 k.launch_cluster_list_xc = &Tile::launch_cluster_list;
                 k.smem_xc = Tile::SMEM;
+                // a cluster of one CTA is a single-CTA tile: a ragged length
+                // class can run it as a launch of its own with the queue
+                if constexpr (LC == 0 && LG == 5 && LW > 0) k.launch_list_dev_xc = &PackedXc<E, LK, LW, MINB>::launch_list_dev;
             }
     }
 };

@@ -83,10 +83,18 @@ void dedicated_entries(int dtype, int stable, int nb, unsigned* mask, int* idx, 
         if (!((*mask >> b) & 1u)) continue;
         int persistent = 0;
         const int e = lookup_default_entry(dtype, stable, 1LL << (kRaggedLmin + b), &persistent);
-        if (e >= 0 && registry()[size_t(e)].lc < 0 && registry()[size_t(e)].launch_list_dev &&
-            registry()[size_t(e)].log2w == kRaggedLmin + b) {
+        const KernelEntry* k = e >= 0 ? &registry()[size_t(e)] : nullptr;
+        // a single-CTA tile with its blocked id-list launch, or (a cluster of
+        // one CTA included) its transposed one when the table picks form 3
+        const bool blocked = k && k->lc < 0 && k->launch_list_dev;
+        const bool xform = k && k->lc <= 0 && persistent == 3 && k->launch_list_dev_xc;
+        if (k && k->log2w == kRaggedLmin + b && (blocked || xform)) {
             idx[b] = e;
-            if (xc) xc[b] = persistent == 3 && registry()[size_t(e)].launch_list_dev_xc;
+            if (xc) xc[b] = xform;
+            else if (!blocked) {  // a caller that does not take the form: no launch it can run
+                idx[b] = -1;
+                *mask &= ~(1u << b);
+            }
         } else {
             *mask &= ~(1u << b);
         }
