@@ -232,6 +232,9 @@ __global__ void __launch_bounds__(S::TPA, MINB) k_sort_packed_xc(const typename 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* sm = reinterpret_cast<R*>(smem_raw);
     const int t = int(threadIdx.x);
+    // programmatic dependent launch (see k_sort_packed)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     for (long long a = blockIdx.x; a < arrays; a += gridDim.x) {
         const long long off = a * (long long)n;
         R v[S::K];

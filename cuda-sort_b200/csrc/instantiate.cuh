@@ -36,14 +36,15 @@ struct Packed {
         if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
         return e;
     }
+    // Programmatic dependent launch: the grid may be scheduled while the
+    // stream's previous kernel drains (the kernel waits for it first).
     static cudaError_t launch(const void* in, void* out, int n, long long arrays, long long grid,
                               cudaStream_t st, unsigned opts) {
         auto fn = k_sort_packed<E, S, CTA, SB>;
         cudaError_t e = prepare<0>(reinterpret_cast<const void*>(fn));
         if (e != cudaSuccess) return e;
-        fn<<<dim3(unsigned(grid)), dim3(CTA), SMEM, st>>>(
-            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), n, arrays, opts);
-        return cudaGetLastError();
+        return launch_pdl(fn, unsigned(grid), CTA, SMEM, st, static_cast<const typename E::Mem*>(in),
+                          static_cast<typename E::Mem*>(out), n, arrays, opts);
     }
     static cudaError_t launch_list(const void* in, void* out, const int* off, const int* ids, int count,
                                    cudaStream_t st) {
@@ -120,6 +121,24 @@ struct Packed {
                            &attrs,  &launch_list,       &launch_pf, -1,   nullptr, &launch_list_dev};
     }
 };
+
+// Launch with programmatic stream serialization allowed (the kernel starts
+// with griddepcontrol.wait, so it still sees all of the previous kernel's
+// writes).
+template <class... P, class... A>
+cudaError_t launch_pdl(void (*fn)(P...), unsigned grid, int cta, size_t smem, cudaStream_t st, A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(unsigned(cta));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, fn, args...);
+}
 
 // Opt in to SMEM bytes of dynamic shared memory for kernel fn (once per
 // device), with a margin for the kernel's own static variables.

@@ -24,9 +24,8 @@ struct PackedXc {
         cudaError_t e = opt_in_smem<SMEM>(reinterpret_cast<const void*>(fn), done);
         if (e != cudaSuccess) return e;
         const long long grid = arrays < 0x7fffffffLL ? arrays : 0x7fffffffLL;
-        fn<<<dim3(unsigned(grid)), dim3(CTA), SMEM, st>>>(static_cast<const typename E::Mem*>(in),
-                                                          static_cast<typename E::Mem*>(out), n, arrays, opts);
-        return cudaGetLastError();
+        return launch_pdl(fn, unsigned(grid), CTA, SMEM, st, static_cast<const typename E::Mem*>(in),
+                          static_cast<typename E::Mem*>(out), n, arrays, opts);
     }
     static cudaError_t launch_list(const void* in, void* out, const int* off, const int* ids, int count,
                                    cudaStream_t st) {

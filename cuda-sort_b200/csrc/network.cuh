@@ -456,6 +456,10 @@ __global__ void __launch_bounds__(CTA) k_sort_packed(const typename E::Mem* in,
     R* nxt = SB ? cur : cur + S::W;
     const int slot = int(threadIdx.x) / S::TPA;
     const int t = int(threadIdx.x) % S::TPA;
+    // programmatic dependent launch: wait for the stream's previous kernel
+    // (immediate when launched without the attribute), then release the next
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     for (long long first = (long long)blockIdx.x * APC; first < arrays;
          first += (long long)gridDim.x * APC) {
         const long long a = first + slot;

@@ -25,12 +25,24 @@ struct Xpose {
     static constexpr size_t SMEM = size_t(WPC) * APW * xp_region<LK, LG>() * sizeof(typename E::Reg);
     static constexpr auto kernel() { return k_sort_xpose<E, LK, LG, WPC, MINB, IO>; }
 
+    // Programmatic dependent launch: the grid may be scheduled while the
+    // stream's previous kernel drains; the kernel waits for that kernel's
+    // completion before its first access (griddepcontrol.wait).
     static cudaError_t launch(const void* in, void* out, int n, long long arrays, cudaStream_t st, unsigned opts) {
         const long long per_cta = (long long)WPC * APW;
         const long long grid = std::min<long long>((arrays + per_cta - 1) / per_cta, 0x7fffffffLL);
-        kernel()<<<dim3(unsigned(grid)), dim3(WPC * 32), SMEM, st>>>(
-            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), n, arrays, opts);
-        return cudaGetLastError();
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(grid));
+        cfg.blockDim = dim3(WPC * 32);
+        cfg.dynamicSmemBytes = SMEM;
+        cfg.stream = st;
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr.val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, kernel(), static_cast<const typename E::Mem*>(in),
+                                  static_cast<typename E::Mem*>(out), n, arrays, opts);
     }
     static cudaError_t attrs(cudaFuncAttributes* a) {
         return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(kernel()));

@@ -376,6 +376,12 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
     const int slot = lane >> LG, t = lane & (G - 1);
     R* sm = reinterpret_cast<R*>(smem_raw) + (warp * APW + slot) * xp_region<LK, LG>();
     const long long stride = (long long)gridDim.x * WPC * APW;
+    // Launched with programmatic stream serialization: wait until the
+    // preceding kernel of the stream has completed and its writes are
+    // visible (immediate without such a predecessor), then let the next
+    // launch's CTAs be scheduled as this grid's CTAs retire.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     // With the sortedness check the tile is loaded in its own order (the
     // striped relabelling would hide the input's order from the test).
     const bool check = (opts & kOptSortedCheck) != 0;
