@@ -12,6 +12,24 @@
 
 namespace b200s {
 
+// Launch with programmatic stream serialization allowed (the kernel starts
+// with griddepcontrol.wait, so it still sees all of the previous kernel's
+// writes).
+template <class... P, class... A>
+cudaError_t launch_pdl(void (*fn)(P...), unsigned grid, int cta, size_t smem, cudaStream_t st, A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(unsigned(cta));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, fn, args...);
+}
+
 // SB: single-buffered shared-memory layers (multi-warp tiles only).
 template <class E, int LK, int LG, int LW, bool SB = false>
 struct Packed {
@@ -108,9 +126,8 @@ struct Packed {
             resident[dev & 63].store(cap, std::memory_order_relaxed);
         }
         const long long g = grid < cap ? grid : cap;
-        fn<<<dim3(unsigned(g)), dim3(CTA), SMEM, st>>>(
-            static_cast<const typename E::Mem*>(in), static_cast<typename E::Mem*>(out), n, arrays, opts);
-        return cudaGetLastError();
+        return launch_pdl(fn, unsigned(g), CTA, SMEM, st, static_cast<const typename E::Mem*>(in),
+                          static_cast<typename E::Mem*>(out), n, arrays, opts);
     }
     static cudaError_t attrs(cudaFuncAttributes* a) {
         return cudaFuncGetAttributes(a, reinterpret_cast<const void*>(k_sort_packed<E, S, CTA, SB>));
@@ -121,24 +138,6 @@ struct Packed {
                            &attrs,  &launch_list,       &launch_pf, -1,   nullptr, &launch_list_dev};
     }
 };
-
-// Launch with programmatic stream serialization allowed (the kernel starts
-// with griddepcontrol.wait, so it still sees all of the previous kernel's
-// writes).
-template <class... P, class... A>
-cudaError_t launch_pdl(void (*fn)(P...), unsigned grid, int cta, size_t smem, cudaStream_t st, A... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(unsigned(cta));
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr;
-    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr.val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = &attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, fn, args...);
-}
 
 // Opt in to SMEM bytes of dynamic shared memory for kernel fn (once per
 // device), with a margin for the kernel's own static variables.

@@ -493,6 +493,9 @@ __global__ void __launch_bounds__(CTA) k_sort_packed_pf(const typename E::Mem* i
     const int t = int(threadIdx.x) % S::TPA;
     const long long stride = (long long)gridDim.x * APC;
     long long first = (long long)blockIdx.x * APC;
+    // programmatic dependent launch (see k_sort_packed)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (first >= arrays) return;  // uniform across the CTA
     R v[S::K];
     {

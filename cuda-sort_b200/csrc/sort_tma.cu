@@ -145,8 +145,19 @@ struct PackedTma {
         if (!status) return cudaErrorInvalidSymbol;
         const long long chunks = (arrays + APC - 1) / APC;
         const long long grid = std::min<long long>(chunks, cap);
-        fn<<<dim3(unsigned(grid)), dim3(CTA), smem, st>>>(tin, tout, n, arrays, rows, status);
-        return cudaGetLastError();
+        // programmatic dependent launch (the kernel waits for the stream's
+        // previous kernel before its first access)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(grid));
+        cfg.blockDim = dim3(CTA);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr.val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, fn, tin, tout, n, arrays, rows, status);
     }
     static TmaEntry entry(int dtype) { return TmaEntry{dtype, E::kStable ? 1 : 0, LK, LG, &launch}; }
 };

@@ -116,6 +116,10 @@ __global__ void __launch_bounds__(CTA) k_sort_packed_tma(const __grid_constant__
     extern __shared__ __align__(1024) unsigned char tma_smem[];
     __shared__ __align__(8) uint64_t full[DEPTH];
 
+    // programmatic dependent launch: the stream's previous kernel has
+    // completed before any access (immediate without such a predecessor)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int tid = int(threadIdx.x);
     const int slot = tid / S::TPA;
     const int t = tid % S::TPA;
