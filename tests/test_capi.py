@@ -87,3 +87,47 @@ def test_tile_table_file_round_trip(tmp_path):
     bad.write_text("0,0,3,9,9,9\n")
     with pytest.raises(bs.B200SortError):
         bs.load_tile_table(str(bad))
+
+
+def _shipped_table():
+    return os.path.join(os.path.dirname(bs.LIB_PATH), "tune", "b200_table.csv")
+
+
+def test_tile_table_rows_name_cluster_tiles_and_forms(tmp_path):
+    # a packed row may give a cluster tile (8th column: log2 CTAs per array)
+    # and launch form 3; the default choice for that length then reports both
+    try:
+        for dtype in (bs.I32_I32, bs.U64_I32):
+            clusters = [t for t in bs.tiles(dtype) if t.log2_ctas > 0]
+            assert clusters, dtype
+            t = clusters[0]
+            w = sum(t.as_tuple())
+            p = tmp_path / ("cluster%d.csv" % dtype)
+            p.write_text("%d,0,%d,%d,%d,%d,3,%d\n" % (dtype, w, t.log2_items, t.log2_lanes, t.log2_warps,
+                                                      t.log2_ctas))
+            assert bs.load_tile_table(str(p)) == 1
+            d = bs.default_tile(dtype, 1 << w)
+            assert (d.as_tuple(), d.persistent) == (t.as_tuple(), 3)
+        # a CTA count no tile of that shape has is rejected
+        t = [t for t in bs.tiles(bs.I32_I32) if t.log2_ctas > 0][0]
+        bad = tmp_path / "bad_ctas.csv"
+        bad.write_text("1,0,%d,%d,%d,%d,3,7\n" % (sum(t.as_tuple()), t.log2_items, t.log2_lanes, t.log2_warps))
+        with pytest.raises(bs.B200SortError):
+            bs.load_tile_table(str(bad))
+        # without the column a row names a single-CTA tile (log2 CTAs 0)
+        one = [t for t in bs.tiles(bs.I32_I32) if t.log2_ctas == 0 and t.log2_warps > 0][0]
+        p = tmp_path / "one.csv"
+        p.write_text("1,0,%d,%d,%d,%d,3\n" % (sum(one.as_tuple()), one.log2_items, one.log2_lanes, one.log2_warps))
+        assert bs.load_tile_table(str(p)) == 1
+        d = bs.default_tile(bs.I32_I32, 1 << sum(one.as_tuple()))
+        assert (d.as_tuple(), d.persistent) == (one.as_tuple(), 3)
+    finally:
+        bs.load_tile_table(_shipped_table())
+
+
+def test_hinted_ragged_sort_checks_its_plan():
+    # a null plan is an argument error, reported before any GPU work
+    fn = bs.declare("b200s_sort_ragged_hinted", ctypes.c_int,
+                    [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                     ctypes.c_int64, ctypes.c_void_p])
+    assert fn(None, None, None, None, None, 1, None) == 1
