@@ -127,7 +127,7 @@ DefaultTable build_defaults() {
 
 struct TableRows {
     std::vector<std::array<int, 4>> packed;  // dtype*2+stable, log2w, registry index, persistent
-    std::vector<std::array<int, 4>> ragged;  // dtype, stable, log2w, family
+    std::vector<std::array<int, 6>> ragged;  // dtype, stable, log2w, family, own tile (registry index or -1), form
 };
 b200s_status parse_table_file(const char* path, TableRows* out);
 void apply_packed_rows(const TableRows& rows, DefaultTable& t);
@@ -135,7 +135,7 @@ std::string shipped_table_path();
 
 }  // namespace
 
-void set_ragged_family(int dtype, int stable, int log2w, int family);
+void set_ragged_family(int dtype, int stable, int log2w, int family, int own_entry, int own_form);
 
 namespace {
 
@@ -146,7 +146,7 @@ DefaultTable& table() {
         TableRows rows;
         if (!path.empty() && std::ifstream(path).good() && parse_table_file(path.c_str(), &rows) == B200S_OK) {
             apply_packed_rows(rows, d);
-            for (const auto& r : rows.ragged) set_ragged_family(r[0], r[1], r[2], r[3]);
+            for (const auto& r : rows.ragged) set_ragged_family(r[0], r[1], r[2], r[3], r[4], r[5]);
         }
         clear_error();
         return d;
@@ -215,7 +215,20 @@ b200s_status parse_table_file(const char* path, TableRows* out) {
             if (!(ss >> tag >> d >> fl >> w >> fam) || !valid_dtype(d) || w < 3 || w > 18 || fam < 0 || fam > 2)
                 return set_error(B200S_ERR_INVALID_ARGUMENT,
                                  "tile table line " + std::to_string(lineno) + ": bad ragged row");
-            out->ragged.push_back({d, effective_stable(d, uint32_t(fl)), w, fam});
+            const int stable = effective_stable(d, uint32_t(fl));
+            // optional tile of the class's own launch (family 2): log2_items,
+            // log2_lanes, log2_warps, form (0 or 3); a single-CTA tile of W
+            int own = -1, form = 0, lk, lg, lw;
+            if (ss >> lk) {
+                if (!(ss >> lg >> lw >> form) || fam != 2 || (form != 0 && form != 3))
+                    return set_error(B200S_ERR_INVALID_ARGUMENT,
+                                     "tile table line " + std::to_string(lineno) + ": bad own-launch tile");
+                own = lookup_tile(d, stable, b200s_tile{lk, lg, lw, 0, 0, 0});
+                if (own < 0 || registry()[size_t(own)].log2w != w || registry()[size_t(own)].lc > 0)
+                    return set_error(B200S_ERR_UNSUPPORTED,
+                                     "tile table line " + std::to_string(lineno) + ": own-launch tile not compiled");
+            }
+            out->ragged.push_back({d, stable, w, fam, own, form});
             continue;
         }
         int d, fl, w, lk, lg, lw, pers = 0, lc = 0;
@@ -267,7 +280,7 @@ int lookup_default_entry(int dtype, int stable, long long n, int* persistent) {
     return lookup_default(dtype, stable, n, persistent);
 }
 
-void set_ragged_family(int dtype, int stable, int log2w, int family);
+void set_ragged_family(int dtype, int stable, int log2w, int family, int own_entry, int own_form);
 
 // The TMA-pipelined kernel for registry entry e and this batch, or null when
 // the batch does not meet its requirements: whole 128-byte rows per array (at
@@ -530,7 +543,7 @@ b200s_status b200s_load_tile_table(const char* path, int32_t* applied) {
         std::lock_guard<std::mutex> lock(g_table_mutex);
         apply_packed_rows(rows, table());
     }
-    for (const auto& r : rows.ragged) set_ragged_family(r[0], r[1], r[2], r[3]);
+    for (const auto& r : rows.ragged) set_ragged_family(r[0], r[1], r[2], r[3], r[4], r[5]);
     if (applied) *applied = int32_t(rows.packed.size() + rows.ragged.size());
     clear_error();
     return B200S_OK;

@@ -38,6 +38,10 @@ namespace {
 std::mutex g_mask_mutex;
 unsigned g_family_mask[4][2] = {};
 unsigned g_dedicated_mask[4][2] = {};
+// the tile of a length class's own launch when its table row names one
+// (registry index + 1; 0: the packed table's tile), and its launch form
+int g_own_entry1[4][2][kMaxBuckets] = {};
+int g_own_form[4][2][kMaxBuckets] = {};
 
 const RaggedEntry* find_ragged(int dtype, int stable) {
     for (const RaggedEntry& e : ragged_registry())
@@ -50,10 +54,12 @@ const RaggedEntry* find_ragged(int dtype, int stable) {
 // Ragged table rows: family 0 (A) or 1 (B) runs the bucket in the persistent
 // kernel with that shape family; family 2 gives the bucket its own launch of
 // the packed tile the tile table chooses for its working length.
-void set_ragged_family(int dtype, int stable, int log2w, int family) {
+void set_ragged_family(int dtype, int stable, int log2w, int family, int own_entry, int own_form) {
     std::lock_guard<std::mutex> lock(g_mask_mutex);
     const int b = log2w - kRaggedLmin;
     if (b < 0 || b >= kMaxBuckets) return;
+    g_own_entry1[dtype][stable][b] = family == 2 && own_entry >= 0 ? own_entry + 1 : 0;
+    g_own_form[dtype][stable][b] = own_form;
     if (family == 1) g_family_mask[dtype][stable] |= 1u << b;
     else g_family_mask[dtype][stable] &= ~(1u << b);
     if (family == 2) g_dedicated_mask[dtype][stable] |= 1u << b;
@@ -82,7 +88,13 @@ void dedicated_entries(int dtype, int stable, int nb, unsigned* mask, int* idx, 
         if (xc) xc[b] = false;
         if (!((*mask >> b) & 1u)) continue;
         int persistent = 0;
-        const int e = lookup_default_entry(dtype, stable, 1LL << (kRaggedLmin + b), &persistent);
+        int e;
+        {
+            std::lock_guard<std::mutex> lock(g_mask_mutex);
+            e = g_own_entry1[dtype][stable][b] - 1;
+            persistent = g_own_form[dtype][stable][b];
+        }
+        if (e < 0) e = lookup_default_entry(dtype, stable, 1LL << (kRaggedLmin + b), &persistent);
         const KernelEntry* k = e >= 0 ? &registry()[size_t(e)] : nullptr;
         // a single-CTA tile with its blocked id-list launch, or (a cluster of
         // one CTA included) its transposed one when the table picks form 3

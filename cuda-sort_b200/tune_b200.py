@@ -38,7 +38,8 @@ import workloads  # noqa: E402
 TARGET_ELEMS = 1 << 22
 FORM_NAMES = {0: "one-shot", 1: "prefetch", 2: "TMA", 3: "transposed"}
 # ragged rows: 0 / 1 run the bucket in the persistent kernel with shape family
-# A / B; 2 gives the bucket its own launch of the tabled tile of its length
+# A / B; 2 gives the bucket a launch of its own, in the tile and form the row
+# names (the tuner searches them)
 FAMILY_NAMES = {0: "persistent A", 1: "persistent B", 2: "own launch"}
 
 
@@ -123,10 +124,9 @@ def tune_ragged(dtype, flags, flush, passes, log, summary):
         ins = [src.clone() for _ in range(sets)]
         outs = [torch.empty_like(src) for _ in range(sets)]
         d_off = torch.from_numpy(off.astype(np.int32)).cuda()
-        res = {}
-        for fam in (0, 1, 2):
+        def time_row(row):
             with tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False) as f:
-                f.write("r,%d,%d,%d,%d\n" % (dtype, flags, L, fam))
+                f.write(row + "\n")
             bs.load_tile_table(f.name)
             os.unlink(f.name)
             plans = [bs.Plan(dtype, arrays, flags) for _ in range(sets)]   # one captured graph per buffer set
@@ -134,17 +134,38 @@ def tune_ragged(dtype, flags, flush, passes, log, summary):
                         for i in range(sets)]
             for fn in launches:
                 fn()   # capture each plan's graph outside the timed passes
-            res[fam] = devtime.batched_us(launches, flush, passes)
+            r = devtime.batched_us(launches, flush, passes)
             for p in plans:
                 p.close()
-            log("ragged dtype=%d flags=%d W=%d family=%d: %.2f us (spread %.1f %%)"
-                % (dtype, flags, 1 << L, fam, res[fam][0], 100 * res[fam][1]))
-        order = sorted(res, key=lambda k: res[k][0])
-        fam, second = order[0], order[1]
-        rows.append("r,%d,%d,%d,%d  # %.2f us (spread %.1f %%) vs %.2f us (%s)"
-                    % (dtype, flags, L, fam, res[fam][0], 100 * res[fam][1], res[second][0], FAMILY_NAMES[second]))
-        summary.append(("ragged", dtype, flags, 1 << L, arrays, FAMILY_NAMES[fam], res[fam][0], res[fam][1],
-                        FAMILY_NAMES[second], res[second][0]))
+            return r
+
+        # families 0 and 1: the persistent kernel; family 2: a launch of its
+        # own, in each single-CTA tile of W and each of its id-list forms
+        # (form 0, and form 3 where compiled; a cluster of one CTA has form 3
+        # only); the row keeps the fastest tile
+        cands = [("r,%d,%d,%d,%d" % (dtype, flags, L, fam), FAMILY_NAMES[fam]) for fam in (0, 1)]
+        for base in bs.tiles(dtype, flags):
+            if sum(base.as_tuple()) != L or base.log2_ctas != 0:
+                continue
+            info = bs.tile_info(dtype, 1 << L, flags, base)
+            forms = ([] if info.arrays_per_cta == 0 else [0]) + ([3] if info.xpose_form else [])
+            for form in forms:
+                cands.append(("r,%d,%d,%d,2,%d,%d,%d,%d" % (dtype, flags, L, base.log2_items, base.log2_lanes,
+                                                             base.log2_warps, form),
+                              "own launch " + _shape(base.with_form(form))))
+        res = []
+        for row, name in cands:
+            us, spread = time_row(row)
+            if us is None:
+                continue
+            log("ragged dtype=%d flags=%d W=%d %s: %.2f us (spread %.1f %%)"
+                % (dtype, flags, 1 << L, name, us, 100 * spread))
+            res.append((us, spread, row, name))
+        res.sort(key=lambda r: r[0])
+        (us, spread, row, name), second = res[0], res[1]
+        time_row(row)   # the class keeps its best row while the next ones are timed
+        rows.append("%s  # %.2f us (spread %.1f %%) vs %.2f us (%s)" % (row, us, 100 * spread, second[0], second[3]))
+        summary.append(("ragged", dtype, flags, 1 << L, arrays, name, us, spread, second[3], second[0]))
         del ins, outs, src
         torch.cuda.empty_cache()
         L += 1
@@ -196,8 +217,8 @@ def main():
                                                          "%Y-%m-%d %H:%M UTC"), bs.version()))
         f.write("# packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps,form (0 one-shot, 1 prefetch, 2 TMA, "
                 "3 transposed)\n")
-        f.write("# ragged rows: r,dtype,flags,log2_w,family (0: persistent, larger per-thread tile; 1: persistent, "
-                "smaller; 2: own launch of the tabled tile)\n")
+        f.write("# ragged rows: r,dtype,flags,log2_w,family[,log2_items,log2_lanes,log2_warps,form] (0: persistent, "
+                "larger per-thread tile; 1: persistent, smaller; 2: a launch of its own, in the tile and form given)\n")
         for ln in lines:
             f.write(ln + "\n")
     if args.summary:

@@ -146,9 +146,10 @@ b200s_status b200s_test_stall_tma_loads(int32_t enable);
 /* Replace rows of the default tile table from a CSV file; '#' starts a
  * comment.  Packed rows: dtype,flags,log2_w,log2_items,log2_lanes,log2_warps
  * [,form[,log2_ctas]] (form: 0 .. 3 as b200s_tile.persistent; log2_ctas: CTAs
- * per array of a cluster tile, default 0).  Ragged rows: r,dtype,flags,log2_w,family (0: the
- * persistent kernel with the larger per-thread tile, 1: with the smaller one, 2: a launch of its own of the
- * packed table's tile for that length), read by plans created afterwards.
+ * per array of a cluster tile, default 0).  Ragged rows: r,dtype,flags,log2_w,family
+ * [,log2_items,log2_lanes,log2_warps,form] (0: the persistent kernel with the larger per-thread tile, 1: with
+ * the smaller one, 2: a launch of its own, in the single-CTA tile and form (0 or 3) given, or without them the
+ * packed table's tile and form for that length), read by plans created afterwards.
  * Returns the number of rows applied in *applied. */
 b200s_status b200s_load_tile_table(const char* path, int32_t* applied);
 

@@ -131,3 +131,27 @@ def test_hinted_ragged_sort_checks_its_plan():
                     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                      ctypes.c_int64, ctypes.c_void_p])
     assert fn(None, None, None, None, None, 1, None) == 1
+
+
+def test_ragged_rows_name_the_tile_of_a_launch_of_its_own(tmp_path):
+    # r,dtype,flags,log2_w,2,log2_items,log2_lanes,log2_warps,form: a
+    # single-CTA tile of W in form 0 or 3; anything else is rejected
+    tiles = [t for t in bs.tiles(bs.I32_I32) if t.log2_ctas == 0 and sum(t.as_tuple()) == 10]
+    assert len(tiles) >= 2
+    try:
+        good = tmp_path / "own.csv"
+        good.write_text("".join("r,1,0,10,2,%d,%d,%d,%d\n" % (t.log2_items, t.log2_lanes, t.log2_warps, f)
+                                for t in tiles for f in (0, 3)))
+        assert bs.load_tile_table(str(good)) == 2 * len(tiles)
+        t = tiles[0]
+        for line in ("r,1,0,10,1,%d,%d,%d,0\n" % (t.log2_items, t.log2_lanes, t.log2_warps),   # not family 2
+                     "r,1,0,10,2,%d,%d,%d,2\n" % (t.log2_items, t.log2_lanes, t.log2_warps),   # form 2
+                     "r,1,0,11,2,%d,%d,%d,0\n" % (t.log2_items, t.log2_lanes, t.log2_warps),   # tile of another W
+                     "r,1,0,10,2,9,9,9,0\n",                                                     # no such tile
+                     "r,1,0,10,2,%d,%d\n" % (t.log2_items, t.log2_lanes)):                      # incomplete
+            bad = tmp_path / "bad_own.csv"
+            bad.write_text(line)
+            with pytest.raises(bs.B200SortError):
+                bs.load_tile_table(str(bad))
+    finally:
+        bs.load_tile_table(_shipped_table())

@@ -216,3 +216,36 @@ def test_hinted_sort_launches_only_the_classes_present(dtype, flags):
         plan.close()
         _route(dtype, flags, [(L, 0) for L in Ls])
         bs.load_tile_table(os.path.join(os.path.dirname(bs.LIB_PATH), "tune", "b200_table.csv"))
+
+
+@pytest.mark.parametrize("dtype,flags", [(bs.I32, 0), (bs.I32_I32, 0), (bs.I32_I32, bs.STABLE), (bs.U64_I32, 0)])
+def test_launch_of_its_own_in_every_named_tile_and_form(dtype, flags):
+    # ragged rows that name the tile and form of a class's own launch: every
+    # single-CTA tile of W = 512 .. 4096 in forms 0 and 3 (where compiled)
+    # gives the oracle's output, graph and direct
+    import os
+    lengths = workloads.ragged_lengths(3000, max_len=4096, seed=41)
+    data, off = workloads.make_ragged(dtype, lengths, "distinct16", seed=41, extremes=True)
+    exp = expected(dtype, flags, data, off)
+    cands = []
+    for t in bs.tiles(dtype, flags):
+        L = sum(t.as_tuple())
+        if t.log2_ctas == 0 and 9 <= L <= 12:
+            info = bs.tile_info(dtype, 1 << L, flags, t)
+            for form in ([0] if info.arrays_per_cta else []) + ([3] if info.xpose_form else []):
+                cands.append((L, t, form))
+    assert cands
+    try:
+        for L, t, form in cands:
+            _own = "r,%d,%d,%d,2,%d,%d,%d,%d" % (dtype, flags, L, t.log2_items, t.log2_lanes, t.log2_warps, form)
+            import tempfile
+            with tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False) as f:
+                f.write(_own + "\n")
+            bs.load_tile_table(f.name)
+            os.unlink(f.name)
+            for mode in ("graph", "direct"):
+                got, too_long = run(dtype, flags, data, off, mode)
+                assert too_long == 0
+                assert np.array_equal(got, exp), (_own, mode)
+    finally:
+        bs.load_tile_table(os.path.join(os.path.dirname(bs.LIB_PATH), "tune", "b200_table.csv"))
