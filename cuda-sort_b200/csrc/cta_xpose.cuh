@@ -38,7 +38,15 @@
 //
 // Cluster stages (index bits above one CTA's slice) keep network.cuh's
 // distributed-shared-memory layers (publish, cluster barrier, read the
-// partner CTA's element, pick); their local merges run as a window chain.
+// partner CTA's element, pick), run in window layout LT: there a warp's lanes
+// read 32 consecutive elements of the partner's slice (in the blocked layout
+// they were 2^LK + 1 elements apart, each read pulling a whole sector), and
+// the registers hold the slice's top LK bits, so the first LK local merges
+// need no layout change; the remaining merges run as a window chain.
+//
+// Keys alone (kKeysOnly) sort each thread's registers with Batcher's odd-even
+// merge sort instead of stages 0 .. LK-1 (xpose.cuh); records keep the
+// reference's comparators throughout.
 #pragma once
 #include <cooperative_groups.h>
 
