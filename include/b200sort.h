@@ -155,7 +155,11 @@ b200s_status b200s_load_tile_table(const char* path, int32_t* applied);
 
 /* Sort `arrays` independent arrays of n elements each, packed back to back
  * (array a at element offset a*n), from d_in into d_out (device pointers; may
- * be equal).  tile == NULL uses the default tile for n. */
+ * be equal).  tile == NULL uses the default tile for n.  The single-CTA
+ * launches allow programmatic stream serialization: their CTAs may be
+ * scheduled while the stream's previous kernel drains, and each waits for
+ * that kernel's completion (griddepcontrol.wait) before touching memory, so
+ * stream order is kept for any producer. */
 b200s_status b200s_sort_packed(b200s_dtype dtype, const void* d_in, void* d_out, int32_t n,
                                int64_t arrays, uint32_t flags, const b200s_tile* tile,
                                void* stream);
